@@ -1,0 +1,429 @@
+#!/usr/bin/env python
+"""Benchmark of the hot path: FP64 Helmholtz solves per second on one or more
+B200s (one process per GPU, independent replicas), plus the reference's CPU
+solver (FISHPACK hw3crt through the reference wrapper) as the baseline arm.
+
+Default workload: 512^3 cells, boundary codes (3, 4, 0), lambda = -1,
+f ~ U[-1, 1] + 1e3 cos(pi x) cos(pi y / 2) cos(2 pi z), Neumann data ~ U[-1, 1]
+(seeded synthetic data with the precision configuration's shapes and value
+distributions).  A step solves a batch of `--batch` such problems, each held in
+its own device array; arrays are larger than L2, so no flush is needed.
+
+usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (nx, ny, nz, xbc, ybc, zbc, lam, description)
+    "helmholtz_fp64_512": (512, 512, 512, 3, 4, 0, -1.0,
+                           "FP64 Helmholtz solve 512^3, BC (3,4,0), lambda=-1, f~U[-1,1]+1e3 smooth mode"),
+    "helmholtz_fp64_256": (256, 256, 256, 1, 3, 0, -4.0,
+                           "FP64 Helmholtz solve 256^3, BC (1,3,0), lambda=-4, f~N(0,1)"),
+    "helmholtz_fp64_128": (128, 128, 128, 1, 2, 0, -2.0,
+                           "FP64 Helmholtz solve 128^3, BC (1,2,0), lambda=-2, manufactured 4-mode u"),
+    "helmholtz_fp64_256x192x320": (256, 192, 320, 2, 4, 3, -7.3,
+                                   "FP64 Helmholtz solve 256x192x320, BC (2,4,3), f~U[-1,1]"),
+}
+DEFAULT_WORKLOAD = "helmholtz_fp64_512"
+METRIC = "solves/s (FP64 Helmholtz solve)"
+
+
+def make_problem(name, seed):
+    from oracle import gen
+    nx, ny, nz, xbc, ybc, zbc, lam, _ = WORKLOADS[name]
+    if name == "helmholtz_fp64_512":
+        return gen.config3_problem(seed=seed, n=nx)
+    if name == "helmholtz_fp64_256":
+        return gen.config5_problem(seed=seed, n=nx)
+    if name == "helmholtz_fp64_128":
+        return gen.config1_problem(seed=seed, n=nx)
+    return gen.random_problem(nx, ny, nz, xbc, ybc, zbc, lam, seed=seed)
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes of the solver schedule (mirrors the host planner)
+# ---------------------------------------------------------------------------
+
+def _windows(bc, n):
+    s, e = {0: (0, n - 1), 1: (1, n - 1), 2: (1, n), 3: (0, n), 4: (0, n - 1)}[bc]
+    sp1 = n + 1 if bc == 0 else e
+    return s, e, s, sp1
+
+
+def solve_pass_bytes(nx, ny, nz, xbc, ybc, zbc, esize=8):
+    """Bytes each line pass of one solve must read and write (algorithmic:
+    every loaded and stored entry once), in launch order."""
+    xs, xe, xp0, xp1 = _windows(xbc, nx)
+    ys, ye, yp0, yp1 = _windows(ybc, ny)
+    zs, ze, zp0, zp1 = _windows(zbc, nz)
+    X, Xs = xe - xs + 1, xp1 - xp0 + 1
+    Y, Ys = ye - ys + 1, yp1 - yp0 + 1
+    Z, Zs = ze - zs + 1, zp1 - zp0 + 1
+    return [
+        (Y * Z) * (X + Xs) * esize,    # x forward: f -> work
+        (Xs * Z) * (Y + Ys) * esize,   # y forward
+        (Xs * Ys) * (Z + Z) * esize,   # z forward + divide + z inverse
+        (Xs * Z) * (Ys + Y) * esize,   # y inverse
+        (Y * Z) * (Xs + X) * esize,    # x inverse: work -> f
+    ]
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_ids):
+        self.gpu_ids = gpu_ids
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", ",".join(self.gpu_ids), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self._t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[4:8]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def nvml_ids_for_visible(devices):
+    """nvidia-smi ids (UUIDs) of the given torch device indices."""
+    import torch
+    out = []
+    for d in devices:
+        try:
+            u = str(torch.cuda.get_device_properties(d).uuid)
+            out.append(u if u.startswith("GPU-") else "GPU-" + u)
+        except Exception:
+            out.append(str(d))
+    return out
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines (reference CPU solver)
+# ---------------------------------------------------------------------------
+
+def cpu_baseline_single(p):
+    from oracle import fishpack
+    if not fishpack.available():
+        return {"value": None, "unit": "solves/s", "cores": 1, "kind": "reference",
+                "sample": "unavailable: fishpack runner not built"}
+    _, best, _ = fishpack.solve(p, repeats=1)
+    return {"value": 1.0 / best, "unit": "solves/s", "cores": 1, "kind": "reference",
+            "seconds_per_solve": best,
+            "sample": f"one {p['nx']}x{p['ny']}x{p['nz']} BC ({p['xbc']},{p['ybc']},{p['zbc']}) solve, "
+                      "FISHPACK hw3crt via the reference's solver_3d, 1 thread"}
+
+
+def run_reference_arm(args):
+    """The reference's CPU implementation of the path on the host cores:
+    concurrent single-threaded hw3crt processes (hw3crt is serial)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import fishpack
+    name = args.workload
+    nx, ny, nz, xbc, ybc, zbc, lam, desc = WORKLOADS[name]
+    if not fishpack.available():
+        print(json.dumps({"impl": "reference", "unavailable": "fishpack runner (oracle/_ref) not built"}))
+        return 0
+    p = make_problem(name, seed=3)
+    cores = os.cpu_count() or 1
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except Exception:
+        avail = 64 << 30
+    per_proc = 3 * (nx + 1) * (ny + 1) * (nz + 1) * 8 + (256 << 20)
+    procs = max(1, min(cores, int(avail * 0.6 // per_proc), args.ref_procs))
+    small = make_problem("helmholtz_fp64_128", seed=1)
+    for _ in range(args.warmup):
+        fishpack.solve_many_parallel(small, procs)  # untimed: warms the binary and page cache
+    times = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ts = fishpack.solve_many_parallel(p, procs)
+        times.append(max(ts))
+    wall = time.perf_counter() - t0
+    total = sum(times)
+    value = procs * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
+        "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": name, "description": desc, "grid": [nx, ny, nz],
+                   "bc": [xbc, ybc, zbc], "lambda": lam, "processes": procs},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": procs, "kind": "reference",
+                         "sample": f"each step: {procs} concurrent {nx}x{ny}x{nz} solves, one "
+                                   "single-threaded FISHPACK hw3crt process per core; warm-up "
+                                   "steps solve 128^3"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": wall,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import cuhelmholtz_b200 as chz
+    from cuhelmholtz_b200 import _lib
+    from oracle.stencil import FACE_KEYS
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        if world == 1 and args.gpus > 1:
+            raise SystemExit("launch N>1 with torch.distributed.run (one process per GPU)")
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    name = args.workload
+    nx, ny, nz, xbc, ybc, zbc, lam, desc = WORKLOADS[name]
+    p = make_problem(name, seed=3 + rank)
+    npts = (nx + 1) * (ny + 1) * (nz + 1)
+    B = args.batch
+    stream = torch.cuda.current_stream()
+
+    # device arrays: B right-hand sides (solved in place), faces, workspace
+    f_host = torch.from_numpy(np.ascontiguousarray(p["f"]).ravel()).pin_memory()
+    u_host = torch.empty_like(f_host).pin_memory()
+    fs = [f_host.to("cuda", non_blocking=False) for _ in range(B)]
+    faces_h = {k: (None if p.get(k) is None else torch.from_numpy(np.ascontiguousarray(p[k]).ravel()).pin_memory())
+               for k in FACE_KEYS}
+    faces = {k: (None if v is None else v.to("cuda")) for k, v in faces_h.items()}
+    dom = p["dom"]
+
+    def solve(f):
+        chz.cuda_helmholtz_solver(dom[0], dom[1], nx, xbc, faces["bcl"], faces["bcr"],
+                                  dom[2], dom[3], ny, ybc, faces["bcb"], faces["bct"],
+                                  dom[4], dom[5], nz, zbc, faces["bcf"], faces["bce"],
+                                  lam, f)
+
+    # accuracy of one solve against the oracle's restatement is covered by the
+    # GPU tests; here we keep one untouched copy to report the relative
+    # residual of the benchmarked solve.
+    for _ in range(args.warmup):
+        for f in fs:
+            solve(f)
+    torch.cuda.synchronize()
+
+    # ---- device-timed throughput ----
+    sampler = ClockSampler(nvml_ids_for_visible([local])) if rank == 0 else None
+    barrier()
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.start()
+        time.sleep(0.15)
+    launches0 = _lib.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        for f in fs:
+            solve(f)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = _lib.launch_count() - launches0
+    elapsed_ms = ev0.elapsed_time(ev1)
+    clocks = sampler.stop() if sampler else None
+    barrier()
+    t = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    elapsed_max_ms = float(t.item())
+    solves = world * args.steps * B
+    value = solves / (elapsed_max_ms / 1000.0)
+    ms_per_step = elapsed_max_ms / args.steps
+
+    # ---- per-kernel times with CUDA events on the launching stream ----
+    _lib.trace_enable(True)
+    tsteps = max(1, min(args.steps, 3))
+    for _ in range(tsteps):
+        for f in fs:
+            solve(f)
+    torch.cuda.synchronize()
+    _lib.trace_enable(False)
+    tr = _lib.trace_collect()
+    pass_bytes = solve_pass_bytes(nx, ny, nz, xbc, ybc, zbc)
+    line_labels = ["solve_x_fwd", "solve_y_fwd", "solve_z_fwd_div_inv", "solve_y_inv", "solve_x_inv"]
+    lp_ms = sum(tr[k][1] for k in line_labels if k in tr)
+    lp_n = sum(tr[k][0] for k in line_labels if k in tr)
+    nsolves_traced = tsteps * B
+    lp_bytes = sum(pass_bytes) * nsolves_traced
+    peak, peak_src = measured_peaks()
+    achieved = (lp_bytes / (lp_ms / 1000.0)) / 1e9 if lp_ms > 0 else None
+    per_pass = {k: {"launches": tr[k][0], "avg_ms": tr[k][1] / tr[k][0],
+                    "gbs": (pass_bytes[i] / (tr[k][1] / tr[k][0] / 1000.0)) / 1e9}
+                for i, k in enumerate(line_labels) if k in tr}
+    total_trace_ms = sum(v[1] for v in tr.values())
+    solve_bytes = sum(pass_bytes)
+
+    # ---- end to end through the public API with host buffers ----
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    esteps = max(1, min(args.steps, args.e2e_steps))
+    face_bytes = sum(v.numel() * 8 for v in faces_h.values() if v is not None)
+    e0.record(stream)
+    for _ in range(esteps):
+        fs[0].copy_(f_host, non_blocking=True)
+        for k, v in faces_h.items():
+            if v is not None:
+                faces[k].copy_(v, non_blocking=True)
+        solve(fs[0])
+        u_host.copy_(fs[0], non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * esteps / (float(t.item()) / 1000.0)
+
+    # ---- accuracy of the benchmarked solve: relative residual (FP64, host) ----
+    rel_residual = None
+    if rank == 0 and args.check:
+        from oracle import stencil
+        u = u_host.numpy().reshape(nz + 1, ny + 1, nx + 1)
+        fc = {k: p.get(k) for k in FACE_KEYS}
+        r = stencil.residual(u, p["f"], nx, ny, nz, xbc, ybc, zbc, p["dom"], lam, fc)
+        rel_residual = float(np.linalg.norm(r) / np.linalg.norm(p["f"]))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_single(p)
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": name, "description": desc, "grid": [nx, ny, nz], "bc": [xbc, ybc, zbc],
+                   "lambda": lam, "batch_per_step": B, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (each right-hand side 1 array per problem, "
+                         f"{npts * 8 / 1e9:.2f} GB each)"},
+        "hbm_gbs_solve": (solve_bytes * args.steps * B / (elapsed_ms / 1000.0)) / 1e9,
+        "algorithmic_bytes_per_solve": solve_bytes,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "kernel": "line_pass<double> (5 launches per solve)",
+                     "peak_source": peak_src, "per_pass": per_pass,
+                     "line_pass_share_of_traced_time": lp_ms / total_trace_ms if total_trace_ms else None,
+                     "launches_traced": lp_n},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "solves/s",
+                "h2d_bytes_per_step": npts * 8 + face_bytes, "d2h_bytes_per_step": npts * 8},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "rel_residual": rel_residual,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--batch", type=int, default=8, help="solves per step (separate arrays)")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--ref-procs", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--check", action="store_true", help="report the residual of the solve")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

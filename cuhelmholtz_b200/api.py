@@ -1,0 +1,136 @@
+"""Python mirror of the reference's interface for the hot path, over the C-ABI.
+
+Same names, argument order and meaning as the reference:
+
+* ``do_transform(d_data, d_out, NX, NY, NZ, X_TRANS, Y_TRANS, Z_TRANS)``
+  (cudasymmfft/funcinterface.h:5-12)
+* ``cuda_helmholtz_solver(left, right, NX, xbc, bcl, bcr, bottom, top, NY, ybc,
+  bcb, bct, front, back, NZ, zbc, bcf, bce, lambda_, f)``
+  (cudahelmholtz/cuda_helmholtz_solver.h:5-11)
+
+Arrays are CUDA float64 torch tensors (device memory; torch is only the
+allocator and stream provider here).  Where the reference ends the process
+(bad boundary code, in-place call on a non-cube, CUDA error) these raise
+:class:`CHZError` with the library's status and message.  Calls are
+stream-ordered on torch's current stream; they do not synchronise.
+"""
+from __future__ import annotations
+
+from typing import Optional
+
+import torch
+
+from . import _lib
+
+# transform_kind, cudasymmfft/global.h:6-15
+DCT_1, DCT_2, DCT_3, DST_1, DST_2, DST_3, DFT_R2C, DFT_C2R = range(8)
+KIND_NAMES = ("DCT_1", "DCT_2", "DCT_3", "DST_1", "DST_2", "DST_3", "DFT_R2C", "DFT_C2R")
+
+CHZ_SUCCESS = 0
+CHZ_ERROR_INVALID_VALUE = 1
+CHZ_ERROR_UNSUPPORTED_SIZE = 2
+CHZ_ERROR_NOT_CUBIC = 3
+CHZ_ERROR_CUDA = 4
+CHZ_ERROR_ALLOC = 5
+CHZ_ERROR_WORKSPACE = 6
+
+
+class CHZError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        self.status = status
+        super().__init__(f"{_lib.lib().chz_status_string(status).decode()}: {message}")
+
+
+def _check(status: int) -> None:
+    if status != CHZ_SUCCESS:
+        raise CHZError(status, _lib.lib().chz_last_error().decode())
+
+
+def _ptr(t: Optional[torch.Tensor], name: str, numel: Optional[int] = None) -> int:
+    if t is None:
+        return 0
+    if not isinstance(t, torch.Tensor):
+        raise TypeError(f"{name} must be a torch tensor")
+    if not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor (device memory)")
+    if t.dtype != torch.float64:
+        raise ValueError(f"{name} must be float64")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if numel is not None and t.numel() < numel:
+        raise ValueError(f"{name} holds {t.numel()} values, needs {numel}")
+    return t.data_ptr()
+
+
+def _stream(stream) -> int:
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, torch.cuda.Stream):
+        return stream.cuda_stream
+    return int(stream)
+
+
+def padded_numel(nx: int, ny: int, nz: int) -> int:
+    return (nx + 2) * (ny + 2) * (nz + 2)
+
+
+def do_transform(d_data: torch.Tensor, d_out: Optional[torch.Tensor], NX: int, NY: int, NZ: int,
+                 X_TRANS: int, Y_TRANS: int, Z_TRANS: int, stream=None,
+                 allow_noncubic_inplace: bool = False) -> torch.Tensor:
+    """3-D mixed transform on the padded (NZ+2, NY+2, NX+2) array.  Returns the
+    tensor holding the result (``d_data`` in place, else ``d_out``)."""
+    n = padded_numel(NX, NY, NZ)
+    p_in = _ptr(d_data, "d_data", n)
+    p_out = _ptr(d_out, "d_out", n) if d_out is not None else 0
+    fn = _lib.lib().chz_do_transform_any if allow_noncubic_inplace else _lib.lib().chz_do_transform
+    _check(fn(p_in, p_out, NX, NY, NZ, int(X_TRANS), int(Y_TRANS), int(Z_TRANS), _stream(stream)))
+    return d_data if (d_out is None or p_out == p_in) else d_out
+
+
+def _face_len(axis: str, nx: int, ny: int, nz: int) -> int:
+    return {"x": (ny + 1) * (nz + 1), "y": (nx + 1) * (nz + 1), "z": (nx + 1) * (ny + 1)}[axis]
+
+
+def cuda_helmholtz_solver(left, right, NX, xbc, bcl, bcr,
+                          bottom, top, NY, ybc, bcb, bct,
+                          front, back, NZ, zbc, bcf, bce,
+                          lambda_, f, stream=None, workspace: Optional[torch.Tensor] = None):
+    """Solves lap_h u + lambda u = f in place on ``f`` ((NZ+1, NY+1, NX+1)
+    float64 CUDA tensor).  Returns 0 like the reference."""
+    n = (NX + 1) * (NY + 1) * (NZ + 1)
+    pf = _ptr(f, "f", n)
+    fx, fy, fz = (_face_len(a, NX, NY, NZ) for a in "xyz")
+    faces = [_ptr(bcl, "bcl", fx), _ptr(bcr, "bcr", fx), _ptr(bcb, "bcb", fy),
+             _ptr(bct, "bct", fy), _ptr(bcf, "bcf", fz), _ptr(bce, "bce", fz)]
+    L = _lib.lib()
+    if workspace is None:
+        st = L.chz_helmholtz_solve(float(left), float(right), NX, xbc, faces[0], faces[1],
+                                   float(bottom), float(top), NY, ybc, faces[2], faces[3],
+                                   float(front), float(back), NZ, zbc, faces[4], faces[5],
+                                   float(lambda_), pf, _stream(stream))
+    else:
+        if not workspace.is_cuda:
+            raise ValueError("workspace must be device memory")
+        st = L.chz_helmholtz_solve_ws(float(left), float(right), NX, xbc, faces[0], faces[1],
+                                      float(bottom), float(top), NY, ybc, faces[2], faces[3],
+                                      float(front), float(back), NZ, zbc, faces[4], faces[5],
+                                      float(lambda_), pf, workspace.data_ptr(),
+                                      workspace.numel() * workspace.element_size(), _stream(stream))
+    _check(st)
+    return 0
+
+
+def workspace_size(NX: int, NY: int, NZ: int, precision: int = 0) -> int:
+    return int(_lib.lib().chz_helmholtz_workspace_size(NX, NY, NZ, precision))
+
+
+def solve_problem(p: dict, f: torch.Tensor, faces: Optional[dict] = None, stream=None):
+    """Convenience: solve a problem dict (keys nx, ny, nz, xbc, ybc, zbc, dom,
+    lam) in place on the device tensor ``f``; ``faces`` maps bcl..bce to device
+    tensors (or None)."""
+    faces = faces or {}
+    d = p["dom"]
+    return cuda_helmholtz_solver(d[0], d[1], p["nx"], p["xbc"], faces.get("bcl"), faces.get("bcr"),
+                                 d[2], d[3], p["ny"], p["ybc"], faces.get("bcb"), faces.get("bct"),
+                                 d[4], d[5], p["nz"], p["zbc"], faces.get("bcf"), faces.get("bce"),
+                                 p["lam"], f, stream=stream)

@@ -1,0 +1,93 @@
+// Internal host-side interfaces shared by the kernel and API translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "chz_device.cuh"
+
+namespace chz {
+
+// Boundary terms of the reference's _3d_bc{1..4}_ini_{x,y,z}_ kernels
+// (_cuda_helmholtz_.inl:70-227), applied while the first solver pass loads f.
+struct BcArgs {
+    int xbc, ybc, zbc;
+    int xs, xe, ys, ye, zs, ze;
+    int nx, ny, nz;
+    double dx, dy, dz, dx2, dy2, dz2;
+    const double* f;  // face values are read from the unmodified input f
+    const double *bcl, *bcr, *bcb, *bct, *bcf, *bce;
+};
+
+// Eigenvalue division of _divide_/_periodic_divide_ (_cuda_helmholtz_.inl:276-421)
+// applied between the forward and inverse transforms of the fused z pass.
+// ex/ey/ez are per-entry tables (2 cos(mode * pidiv + shift) - 2) * d^2.
+struct DivArgs {
+    const double* ex;
+    const double* ey;
+    const double* ez;
+    double lambda;
+    int perturb;               // zero the (0,0,0) mode
+    int xz_hi, yz_hi, zz_hi;   // entry indices <= these belong to mode 0
+    int lo, hi;                // spectral window along the line
+};
+
+struct PassArgs {
+    int kind;    // transform of the pass
+    int kind2;   // >= 0: divide, then this inverse transform, in the same pass
+    int u0, nu;  // lines: u in [u0, u0+nu), tiled by W per CTA
+    int v0;      // v = v0 + blockIdx.y
+    long long in_su, in_sv, in_sl;
+    int ld_lo, ld_hi;  // loaded part of the input window (rest is zero)
+    long long out_su, out_sv, out_sl;
+    int st_lo, st_hi;  // stored part of the output window
+    double scale;
+    int use_scale;
+    int PR;       // real-view pitch (>= W)
+    int log2W;
+    int has_bc;
+    int has_div;
+    BcArgs bc;
+    DivArgs dv;
+};
+
+struct LineGeom {
+    int N, M, W, log2W, PR;
+    size_t buf_elems;   // elements of T per buffer
+    size_t smem_bytes;
+    int threads;
+};
+
+// Device tables for one line length and precision (cached for the process).
+struct DeviceLineTables {
+    int N = 0, M = 0;
+    RadixPlan rp{};
+    void* twM = nullptr;
+    void* twN = nullptr;
+    void* tw4N = nullptr;
+    void* inv4sin = nullptr;
+};
+
+// Returns 0 on success; fills `out` with device pointers (cached).
+int get_line_tables(int N, int is_double, int device, DeviceLineTables* out);
+int factor_radices(int M, RadixPlan* rp);
+bool radix_plan_is_pow2(const RadixPlan& rp);
+LineGeom line_geometry(int N, int is_double, bool contig);
+
+// Launchers (return cudaError_t as int).
+enum IoType { kIoF64 = 0, kIoF32 = 1 };
+int launch_line_pass(int is_double, int in_type, int out_type, bool contig, const void* in,
+                     void* out, const PassArgs& a, const DeviceLineTables& tb,
+                     const LineGeom& g, int nv, cudaStream_t stream, const char* label);
+
+// Launch tracing: with tracing on, every kernel launch is bracketed by CUDA
+// events recorded on its own stream; trace_collect() waits for them and
+// reports per-label totals.  launch_count() counts every launch of this library.
+void trace_begin(cudaStream_t stream, const char* label);
+void trace_end(cudaStream_t stream);
+unsigned long long launch_count();
+void count_launch();
+int launch_periodic_fixup(double* f, int nx, int ny, int nz, int xbc, int ybc, int zbc,
+                          cudaStream_t stream);
+
+}  // namespace chz

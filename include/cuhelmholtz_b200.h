@@ -1,0 +1,116 @@
+/*
+ * cuhelmholtz_b200 -- C ABI of the B200-native (sm_100a) 3-D mixed
+ * DFT/DST/DCT transform and FFT-diagonalised Helmholtz solver.
+ *
+ * Every entry point takes plain device pointers, sizes and an optional CUDA
+ * stream handle (`void*` holding a cudaStream_t; NULL = legacy default stream),
+ * returns a chz_status code instead of exiting the process, and is
+ * stream-ordered: it enqueues work and returns without synchronising.
+ *
+ * Layouts (identical to the reference's):
+ *   transform array : (NZ+2)(NY+2)(NX+2) doubles, [z][y][x], rows of NX+2
+ *                     (cudasymmfft/funcinterface.cu:48-83 plan strides)
+ *   solver f        : (NZ+1)(NY+1)(NX+1) doubles, [z][y][x], in place
+ *                     (cudahelmholtz/cuda_helmholtz_solver.cu:178-179)
+ *   Neumann faces   : x faces (NZ+1)(NY+1) [z][y], y faces (NZ+1)(NX+1) [z][x],
+ *                     z faces (NY+1)(NX+1) [y][x]; NULL where the boundary
+ *                     code does not read them (testgpurectangle.cu:46-57)
+ *
+ * The C++-linkage drop-in signatures of the reference live in funcinterface.h
+ * and cuda_helmholtz_solver.h next to this header.
+ */
+#ifndef CUHELMHOLTZ_B200_H_
+#define CUHELMHOLTZ_B200_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum chz_status {
+    CHZ_SUCCESS = 0,
+    CHZ_ERROR_INVALID_VALUE = 1,    /* bad size, boundary code, kind or NULL pointer */
+    CHZ_ERROR_UNSUPPORTED_SIZE = 2, /* N odd, < 4, > 2048, or N/2 has a prime factor > 13 */
+    CHZ_ERROR_NOT_CUBIC = 3,        /* in-place do_transform on a non-cubic grid */
+    CHZ_ERROR_CUDA = 4,             /* a CUDA runtime call failed */
+    CHZ_ERROR_ALLOC = 5,            /* device allocation failed */
+    CHZ_ERROR_WORKSPACE = 6         /* caller workspace too small or misaligned */
+} chz_status;
+
+/* transform kinds: same values as the reference's enum transform_kind
+ * (cudasymmfft/global.h:6-15). */
+enum {
+    CHZ_DCT_1 = 0, CHZ_DCT_2 = 1, CHZ_DCT_3 = 2, CHZ_DST_1 = 3,
+    CHZ_DST_2 = 4, CHZ_DST_3 = 5, CHZ_DFT_R2C = 6, CHZ_DFT_C2R = 7
+};
+
+/* Library version, major * 10000 + minor * 100 + patch. */
+int chz_version(void);
+
+/* Human-readable name of a status code. */
+const char* chz_status_string(int status);
+
+/* Detail of the last error raised on the calling host thread ("" if none). */
+const char* chz_last_error(void);
+
+/* 3-D mixed transform (replaces do_transform, cudasymmfft/funcinterface.cu:25-40).
+ * d_out == NULL or d_out == d_data: in place, the grid must be a cube
+ * (CHZ_ERROR_NOT_CUBIC otherwise, where the reference exits).  Otherwise the
+ * result is written to d_out and d_data is left unchanged (the reference uses
+ * d_data as scratch).  Entries outside each kind's output window are not
+ * written. */
+int chz_do_transform(double* d_data, double* d_out, int nx, int ny, int nz,
+                     int x_kind, int y_kind, int z_kind, void* stream);
+
+/* Same transform without the cubic restriction on in-place calls. */
+int chz_do_transform_any(double* d_data, double* d_out, int nx, int ny, int nz,
+                         int x_kind, int y_kind, int z_kind, void* stream);
+
+/* Device workspace the solver needs for these sizes (bytes).
+ * precision: 0 = FP64 solve, 1 = FP32 + FP64-refinement solve. */
+size_t chz_helmholtz_workspace_size(int nx, int ny, int nz, int precision);
+
+/* Helmholtz solve  lap_h u + lambda u = f  (replaces cuda_helmholtz_solver,
+ * cudahelmholtz/cuda_helmholtz_solver.cu:33-380), FP64, in place on f.
+ * Uses a library-owned workspace cached per (device, stream). */
+int chz_helmholtz_solve(double left, double right, int nx, int xbc,
+                        const double* bcl, const double* bcr,
+                        double bottom, double top, int ny, int ybc,
+                        const double* bcb, const double* bct,
+                        double front, double back, int nz, int zbc,
+                        const double* bcf, const double* bce,
+                        double lambda, double* f, void* stream);
+
+/* As chz_helmholtz_solve with a caller-owned device workspace of at least
+ * chz_helmholtz_workspace_size(nx, ny, nz, 0) bytes, 256-byte aligned. */
+int chz_helmholtz_solve_ws(double left, double right, int nx, int xbc,
+                           const double* bcl, const double* bcr,
+                           double bottom, double top, int ny, int ybc,
+                           const double* bcb, const double* bct,
+                           double front, double back, int nz, int zbc,
+                           const double* bcf, const double* bce,
+                           double lambda, double* f,
+                           void* workspace, size_t workspace_bytes, void* stream);
+
+/* Releases the library-owned workspaces and cached tables of the current
+ * device (after synchronising it). */
+int chz_release_cached(void);
+
+/* Launch tracing (the reference's per-stage host timers, TIME_TEST blocks in
+ * cudasymmfft/dst1funcinplace.cu:21-47, replaced by CUDA events).  With
+ * tracing on, every kernel launch of this library is bracketed by CUDA events
+ * recorded on its own stream.  chz_trace_collect waits for them, writes one
+ * line "label launches total_ms" per kernel label into buf (NUL-terminated,
+ * truncated to len), clears the records and returns the number of launches
+ * collected (-1 on a CUDA error). */
+int chz_trace_enable(int on);
+int chz_trace_collect(char* buf, size_t len);
+
+/* Number of kernel launches this library has issued in this process. */
+unsigned long long chz_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUHELMHOLTZ_B200_H_ */
