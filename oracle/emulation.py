@@ -12,9 +12,11 @@ conventions for the reference's plans:
   0..N/2 interleaved at 0..N+1, unnormalised.
 
 Each kind's result is then restricted to its output window (entries outside are
-NaN), and lines the reference's pre/post kernels do not visit (other-axis index
-N+1) become NaN for the kinds that have pre/post kernels.  A comparison against
-this oracle therefore covers exactly the entries the reference defines.
+NaN), lines the reference's pre/post kernels do not visit (other-axis index
+N+1) become NaN for the kinds that have pre/post kernels, and a line whose
+input window holds an undefined entry defines nothing.  The defined entries of
+a 3-D result are thus the product of the per-axis windows, and a comparison
+against this oracle covers exactly the entries the reference defines.
 """
 from __future__ import annotations
 
@@ -42,6 +44,19 @@ def out_window(kind: int, n: int) -> tuple[int, int]:
     return _OUT_WINDOW[kind](n)
 
 
+# Input window [lo, hi] each kind reads (from the pre kernels' loads and the
+# cuFFT plan lengths).
+_IN_WINDOW = {
+    DST_1: lambda n: (1, n - 1), DST_2: lambda n: (1, n), DST_3: lambda n: (0, n),
+    DCT_1: lambda n: (0, n), DCT_2: lambda n: (0, n - 1), DCT_3: lambda n: (0, n - 1),
+    DFT_R2C: lambda n: (0, n - 1), DFT_C2R: lambda n: (0, n + 1),
+}
+
+
+def in_window(kind: int, n: int) -> tuple[int, int]:
+    return _IN_WINDOW[kind](n)
+
+
 def _c2r(p: np.ndarray, n: int) -> np.ndarray:
     """cuFFT Z2D of length n in place on rows of n+2 doubles."""
     c = p[..., 0:n + 2:2] + 0j
@@ -59,6 +74,10 @@ def _r2c(p: np.ndarray, n: int) -> np.ndarray:
     out = np.empty(p.shape)
     out[..., 0:n + 2:2] = x.real
     out[..., 1:n + 2:2] = x.imag
+    # pocketfft returns exact zeros for the imaginary parts of bins 0 and N/2
+    # even when the input holds NaN; an undefined input defines nothing.
+    bad = np.isnan(p[..., :n]).any(axis=-1)
+    out[bad] = np.nan
     return out
 
 
@@ -246,10 +265,21 @@ def emulate_kind(lines: np.ndarray, kind: int, n: int) -> np.ndarray:
         raise ValueError("rows must hold n+2 entries")
     if n < 2 or n % 2:
         raise ValueError("n must be even and >= 2")
-    out = _KIND_FN[kind](np.asarray(lines, dtype=np.float64), n)
+    lines = np.asarray(lines, dtype=np.float64)
+    out = _KIND_FN[kind](lines, n)
     lo, hi = out_window(kind, n)
     out[..., :lo] = np.nan
     out[..., hi + 1:] = np.nan
+    # A line whose input is undefined defines nothing, not even the constant
+    # zero the DST kinds write at index 0 (such lines lie outside the product
+    # of the per-axis windows, where the reference holds meaningless values).
+    ilo, ihi = in_window(kind, n)
+    used = lines[..., ilo:ihi + 1]
+    if kind == DFT_C2R:  # the imaginary parts of bins 0 and N/2 are not read
+        keep = np.ones(ihi - ilo + 1, dtype=bool)
+        keep[[1, n + 1]] = False
+        used = used[..., keep]
+    out[np.isnan(used).any(axis=-1)] = np.nan
     return out
 
 
