@@ -120,6 +120,12 @@ def cuda_helmholtz_solver(left, right, NX, xbc, bcl, bcr,
     return 0
 
 
+def set_kernel_family(generic_only: bool) -> bool:
+    """Selects the register-resident kernels (default) or the generic
+    mixed-radix kernel for every length; returns the previous setting."""
+    return bool(_lib.lib().chz_set_kernel_family(1 if generic_only else 0))
+
+
 def workspace_size(NX: int, NY: int, NZ: int, precision: int = 0) -> int:
     return int(_lib.lib().chz_helmholtz_workspace_size(NX, NY, NZ, precision))
 

@@ -1,0 +1,440 @@
+// Register-resident line-pass kernel for power-of-two half lengths
+// M = N/2 in {16, 32, 64, 128, 256, 512}.
+//
+// Each line is transformed by P = M/16 threads; every thread keeps 16 complex
+// values in registers and performs radix-16 butterflies (radix 2/4/8 for the
+// last factor) between shared-memory exchanges (Stockham order).  The kind's
+// pre step is fused into the first stage's shared-memory reads, the post step
+// reads only the partner values each output needs, and in the fused solver
+// pass the eigenvalue division is applied while the forward post step writes.
+// One shared buffer of (N+2) x (W+1) values holds, in turn, the real input
+// line view, the complex FFT view and the real output view; phases are
+// separated by barriers.
+#pragma once
+#include "chz_device.cuh"
+#include "chz_internal.h"
+
+namespace chz {
+namespace fast {
+
+constexpr int kNT = 128;  // threads per CTA
+constexpr int kR = 16;    // complex values per thread
+
+template <int M>
+struct Cfg {
+    static constexpr int P = M / kR;      // threads per line
+    static constexpr int W = kNT / P;     // lines per CTA
+    static constexpr int N = 2 * M;
+    static constexpr int L = N + 2;       // padded line
+    static constexpr int PR = W + 1;      // real-view pitch (odd: conflict-free transposed access)
+    static constexpr int A16 = (M >= 256) ? 2 : 1;               // radix-16 stages
+    static constexpr int R0 = M / (A16 == 2 ? 256 : 16);          // last radix (1 = none)
+    static constexpr int NST = A16 + (R0 > 1 ? 1 : 0);
+    static constexpr int BUF = L * PR;     // >= 2*M*W
+    static constexpr int RED = P * W;      // DCT1 odd-sum partials
+};
+
+#define CHZ_C1 0.92387953251128675613
+#define CHZ_S1 0.38268343236508977173
+
+template <typename T>
+__device__ __forceinline__ C2<T> cmulc(C2<T> a, T wr, T wi) {
+    return mk<T>(a.x * wr - a.y * wi, a.x * wi + a.y * wr);
+}
+
+// forward radix-16 DFT (4 x 4 with internal twiddles) on v[0..15]
+template <typename T>
+__device__ __forceinline__ void dft16(C2<T>* v) {
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) dft4<T>(v[n2], v[4 + n2], v[8 + n2], v[12 + n2]);
+    const T c1 = T(CHZ_C1), s1 = T(CHZ_S1), r = T(CHZ_SQRT_HALF);
+    // v[n2 + 4 k1] *= w16^(n2 k1)
+    v[5] = cmulc<T>(v[5], c1, -s1);    // t = 1
+    v[6] = cmulc<T>(v[6], r, -r);      // t = 2
+    v[7] = cmulc<T>(v[7], s1, -c1);    // t = 3
+    v[9] = cmulc<T>(v[9], r, -r);      // t = 2
+    v[10] = cmul_negi<T>(v[10]);       // t = 4
+    v[11] = cmulc<T>(v[11], -r, -r);   // t = 6
+    v[13] = cmulc<T>(v[13], s1, -c1);  // t = 3
+    v[14] = cmulc<T>(v[14], -r, -r);   // t = 6
+    v[15] = cmulc<T>(v[15], -c1, s1);  // t = 9
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) dft4<T>(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
+    // v[4 k1 + k2] = X[k1 + 4 k2]: transpose 4 x 4
+    C2<T> t[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) t[i] = v[i];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1)
+#pragma unroll
+        for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = t[4 * k1 + k2];
+}
+
+template <typename T, int r>
+__device__ __forceinline__ void dft_r(C2<T>* v) {
+    if constexpr (r == 16) dft16<T>(v);
+    else if constexpr (r == 8) Dft<T, 8>::run(v, nullptr, 0);
+    else if constexpr (r == 4) Dft<T, 4>::run(v, nullptr, 0);
+    else if constexpr (r == 2) Dft<T, 2>::run(v, nullptr, 0);
+}
+
+// Radix and Ns (product of the previous radices) of stage S.
+template <int M, int S>
+struct StageOf {
+    static constexpr int r = (S < Cfg<M>::A16) ? 16 : Cfg<M>::R0;
+    static constexpr int Ns = (S == 0) ? 1 : (S == 1 ? 16 : 256);
+};
+
+// Stockham butterfly bookkeeping for slot `slot`, butterfly b of stage S.
+template <int M, int S>
+struct Bfly {
+    static constexpr int r = StageOf<M, S>::r;
+    static constexpr int Ns = StageOf<M, S>::Ns;
+    static constexpr int B = kR / r;
+    static constexpr int nb = M / r;
+    __device__ static __forceinline__ int j(int slot, int b) { return slot * B + b; }
+    __device__ static __forceinline__ int in_idx(int slot, int b, int k) { return j(slot, b) + k * nb; }
+    __device__ static __forceinline__ int out_idx(int slot, int b, int k) {
+        const int jj = j(slot, b);
+        const int p = jj & (Ns - 1);
+        return (jj - p) * r + p + k * Ns;
+    }
+};
+
+// Multiply by the stage twiddles and run the radix-r butterflies.
+template <typename T, int M, int S>
+__device__ __forceinline__ void stage_compute(C2<T>* v, int slot, const C2<T>* __restrict__ twM) {
+    using BF = Bfly<M, S>;
+    constexpr int r = BF::r;
+#pragma unroll
+    for (int b = 0; b < BF::B; ++b) {
+        if constexpr (BF::Ns > 1) {
+            const int p = BF::j(slot, b) & (BF::Ns - 1);
+            constexpr int tstep = M / (BF::Ns * r);
+#pragma unroll
+            for (int k = 1; k < r; ++k) v[b * r + k] = cmul<T>(v[b * r + k], ldtw<T>(twM + p * k * tstep));
+        }
+        dft_r<T, r>(v + b * r);
+    }
+}
+
+// Complex value A[n] fed to the FFT, computed from the real view (pre step).
+template <typename T>
+__device__ __forceinline__ C2<T> pre_value(int kind, const T* __restrict__ Rv, int PR, int c, int n,
+                                           int N, int M, const LineTables<T>& tb) {
+    if (kind_is_forward_type(kind)) {
+        return mk<T>(fwd_gather<T>(kind, Rv, PR, c, 2 * n, N, M), fwd_gather<T>(kind, Rv, PR, c, 2 * n + 1, N, M));
+    }
+    const C2<T> vk = inv_spectrum<T>(kind, Rv, PR, c, n, N, M, tb);
+    const C2<T> vm = inv_spectrum<T>(kind, Rv, PR, c, M - n, N, M, tb);
+    const C2<T> wk = ldtw<T>(tb.twN + n);
+    const C2<T> e = cadd<T>(vk, cconj<T>(vm));
+    const C2<T> o = cmul<T>(cconj<T>(wk), csub<T>(vk, cconj<T>(vm)));
+    return cconj<T>(cadd<T>(e, cmul_i<T>(o)));
+}
+
+// Sink for real outputs of the post step: optional division by the
+// Helmholtz eigenvalue (fused z pass) while writing the real view.
+template <typename T>
+struct OutSink {
+    T* Rv;
+    int PR, c;
+    int div;          // apply the division
+    double exy, lam;  // ex[i] + ey[j], lambda
+    const double* ez;
+    int dlo, dhi;     // spectral window along the line
+    int zero_line;    // (i, j) is in the zero-mode set; zero entries l <= zz_hi
+    int zz_hi;
+    __device__ __forceinline__ void put(int l, T val) const {
+        if (div && l >= dlo && l <= dhi) {
+            const double den = (exy + __ldg(ez + l)) + lam;
+            double eig = __drcp_rn(den);
+            if (zero_line && l <= zz_hi) eig = 0.0;
+            val = (T)((double)val * eig);
+        }
+        Rv[l * PR + c] = val;
+    }
+};
+
+// One complete real transform of the W lines held in `buf` (real view in,
+// real view out), for compile-time M and runtime kind.
+template <typename T, int M>
+__device__ __forceinline__ void transform_lines(int kind, T* buf, T* red, int c, int slot,
+                                                const LineTables<T>& tb, const OutSink<T>& sink) {
+    using CF = Cfg<M>;
+    constexpr int W = CF::W, PR = CF::PR, N = CF::N, P = CF::P;
+    C2<T>* Z = reinterpret_cast<C2<T>*>(buf);
+    C2<T> v[kR];
+
+    // DCT1: partial sums of the odd entries x[1], x[3], ..., x[N-1]
+    if (kind == kDCT1) {
+        T acc = T(0);
+#pragma unroll
+        for (int q = 0; q < M / P; ++q) acc += buf[(2 * (slot + q * P) + 1) * PR + c];
+        red[slot * W + c] = acc;
+    }
+
+    // ---- stage 0: pre step fused into the reads ----
+    {
+        using BF = Bfly<M, 0>;
+#pragma unroll
+        for (int k = 0; k < kR; ++k) v[k] = pre_value<T>(kind, buf, PR, c, BF::in_idx(slot, 0, k), N, M, tb);
+        __syncthreads();
+        stage_compute<T, M, 0>(v, slot, tb.twM);
+    }
+
+    // ---- middle and last stages ----
+    // Writes the previous stage's results, then reads this stage's inputs.
+#define CHZ_STAGE(S)                                                                          \
+    if constexpr (CF::NST > S) {                                                              \
+        using PB = Bfly<M, S - 1>;                                                            \
+        _Pragma("unroll") for (int b = 0; b < PB::B; ++b)                                     \
+            _Pragma("unroll") for (int k = 0; k < PB::r; ++k)                                 \
+                Z[PB::out_idx(slot, b, k) * W + c] = v[b * PB::r + k];                        \
+        __syncthreads();                                                                      \
+        using BF = Bfly<M, S>;                                                                \
+        _Pragma("unroll") for (int b = 0; b < BF::B; ++b)                                     \
+            _Pragma("unroll") for (int k = 0; k < BF::r; ++k)                                 \
+                v[b * BF::r + k] = Z[BF::in_idx(slot, b, k) * W + c];                         \
+        __syncthreads();                                                                      \
+        stage_compute<T, M, S>(v, slot, tb.twM);                                              \
+    }
+    CHZ_STAGE(1)
+    CHZ_STAGE(2)
+#undef CHZ_STAGE
+
+    // ---- post step ----
+    using LB = Bfly<M, CF::NST - 1>;
+    if (kind_is_forward_type(kind) || kind == kDCT1 || kind == kDST1) {
+        // publish Z, then read the partner entries
+#pragma unroll
+        for (int b = 0; b < LB::B; ++b)
+#pragma unroll
+            for (int k = 0; k < LB::r; ++k) Z[LB::out_idx(slot, b, k) * W + c] = v[b * LB::r + k];
+        __syncthreads();
+    }
+    if (kind_is_forward_type(kind)) {
+        // split: V[m] = 1/2 (Z[m] + conj Z[M-m]) - i/2 w^m (Z[m] - conj Z[M-m])
+        C2<T> vM = mk<T>(T(0), T(0));
+#pragma unroll
+        for (int b = 0; b < LB::B; ++b)
+#pragma unroll
+            for (int k = 0; k < LB::r; ++k) {
+                const int m = LB::out_idx(slot, b, k);
+                const C2<T> zk = v[b * LB::r + k];
+                const C2<T> zm = Z[((M - m) & (M - 1)) * W + c];
+                const C2<T> wk = ldtw<T>(tb.twN + m);
+                const C2<T> e = cadd<T>(zk, cconj<T>(zm));
+                const C2<T> o = cmul<T>(wk, csub<T>(zk, cconj<T>(zm)));
+                v[b * LB::r + k] = mk<T>(T(0.5) * (e.x + o.y), T(0.5) * (e.y - o.x));
+                if (m == 0) vM = mk<T>(zk.x - zk.y, T(0));
+            }
+        __syncthreads();
+#pragma unroll
+        for (int b = 0; b < LB::B; ++b)
+#pragma unroll
+            for (int k = 0; k < LB::r; ++k) {
+                const int m = LB::out_idx(slot, b, k);
+                const C2<T> V = v[b * LB::r + k];
+                if (kind == kR2C) {
+                    sink.put(2 * m, V.x);
+                    sink.put(2 * m + 1, m == 0 ? T(0) : V.y);
+                    if (m == 0) {
+                        sink.put(N, vM.x);
+                        sink.put(N + 1, T(0));
+                    }
+                } else {
+                    const C2<T> a = cmul<T>(ldtw<T>(tb.tw4N + m), V);
+                    if (kind == kDCT2) {
+                        sink.put(m, a.x);
+                        if (m > 0) sink.put(N - m, -a.y);
+                    } else {  // DST2
+                        sink.put(N - m, a.x);
+                        if (m > 0) sink.put(m, -a.y);
+                        else sink.put(0, T(0));
+                    }
+                    if (m == 0) {
+                        const C2<T> aM = cmul<T>(ldtw<T>(tb.tw4N + M), vM);
+                        sink.put(M, aM.x);
+                    }
+                }
+            }
+    } else if (kind == kDCT1 || kind == kDST1) {
+        // v[n] = Re conj(Z[n/2]) (n even), Im conj(Z[n/2]) (n odd); pairs (k, N-k)
+        T outs[2 * kR];
+        T S = T(0);
+        if (kind == kDCT1 && slot == 0) {
+#pragma unroll
+            for (int q = 0; q < P; ++q) S += red[q * W + c];
+        }
+        T extra = T(0);  // out[N] (DCT1, m = 0)
+#pragma unroll
+        for (int b = 0; b < LB::B; ++b)
+#pragma unroll
+            for (int k = 0; k < LB::r; ++k) {
+                const int m = LB::out_idx(slot, b, k);
+                const C2<T> z = v[b * LB::r + k];
+                const T ve = z.x, vo = -z.y;  // v[2m], v[2m+1]
+                // k = 2m
+                T oe;
+                if (m == 0) {
+                    if (kind == kDCT1) {
+                        const T h = T(0.5) * ve;
+                        oe = h + S;
+                        extra = h - S;
+                    } else {
+                        oe = T(0);
+                    }
+                } else {
+                    const T pe = Z[(M - m) * W + c].x;  // v[N-2m]
+                    const T is4 = ldr<T>(tb.inv4sin + (2 * m <= M ? 2 * m : N - 2 * m));
+                    if (kind == kDCT1) oe = ((ve + pe) * T(0.5) - (ve - pe) * is4) * T(0.5);
+                    else oe = ((ve + pe) * is4 + (ve - pe) * T(0.5)) * T(0.5);
+                }
+                // k = 2m + 1
+                const T po = -Z[(M - m - 1) * W + c].y;  // v[N-2m-1]
+                const int ko = 2 * m + 1;
+                const T is4o = ldr<T>(tb.inv4sin + (ko <= M ? ko : N - ko));
+                T oo;
+                if (kind == kDCT1) oo = ((vo + po) * T(0.5) - (vo - po) * is4o) * T(0.5);
+                else oo = ((vo + po) * is4o + (vo - po) * T(0.5)) * T(0.5);
+                outs[2 * (b * LB::r + k)] = oe;
+                outs[2 * (b * LB::r + k) + 1] = oo;
+            }
+        __syncthreads();
+#pragma unroll
+        for (int b = 0; b < LB::B; ++b)
+#pragma unroll
+            for (int k = 0; k < LB::r; ++k) {
+                const int m = LB::out_idx(slot, b, k);
+                sink.put(2 * m, outs[2 * (b * LB::r + k)]);
+                sink.put(2 * m + 1, outs[2 * (b * LB::r + k) + 1]);
+                if (m == 0 && kind == kDCT1) sink.put(N, extra);
+            }
+    } else {
+        // C2R, DCT3, DST3: outputs come straight from the thread's own values
+        __syncthreads();
+#pragma unroll
+        for (int b = 0; b < LB::B; ++b)
+#pragma unroll
+            for (int k = 0; k < LB::r; ++k) {
+                const int m = LB::out_idx(slot, b, k);
+                const C2<T> z = v[b * LB::r + k];
+                const T v0 = z.x, v1 = -z.y;
+                const int e0 = 2 * m, e1 = 2 * m + 1;
+                if (kind == kC2R) {
+                    sink.put(e0, v0);
+                    sink.put(e1, v1);
+                } else if (kind == kDCT3) {
+                    sink.put(e0 < M ? 2 * e0 : 2 * (N - 1 - e0) + 1, T(0.5) * v0);
+                    sink.put(e1 < M ? 2 * e1 : 2 * (N - 1 - e1) + 1, T(0.5) * v1);
+                } else {  // DST3
+                    if (e0 < M) sink.put(2 * e0 + 1, T(0.5) * v0);
+                    else sink.put(2 * (N - 1 - e0) + 2, T(-0.5) * v0);
+                    if (e1 < M) sink.put(2 * e1 + 1, T(0.5) * v1);
+                    else sink.put(2 * (N - 1 - e1) + 2, T(-0.5) * v1);
+                    if (m == 0) sink.put(0, T(0));
+                }
+            }
+    }
+    __syncthreads();
+}
+
+template <typename TI>
+__device__ __forceinline__ double ldin(const TI* p) { return (double)__ldg(p); }
+
+template <typename T, typename TI, typename TO, int M, bool CONTIG>
+__global__ void __launch_bounds__(kNT, 4)
+fast_line_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tb) {
+    using CF = Cfg<M>;
+    constexpr int W = CF::W, PR = CF::PR, N = CF::N;
+    __shared__ __align__(16) T buf[CF::BUF];
+    __shared__ T red[CF::RED];
+
+    const int t = threadIdx.x;
+    const int c = t % W;
+    const int slot = t / W;
+    const int ub = a.u0 + blockIdx.x * W;
+    const int nl = min(W, a.u0 + a.nu - ub);
+    const int v = a.v0 + blockIdx.y;
+
+    // ---- load the input window ----
+    {
+        int lo, hi;
+        kind_in_window(a.kind, N, lo, hi);
+        const long long vb = (long long)v * a.in_sv;
+        if (CONTIG) {
+            for (int cc = 0; cc < W; ++cc) {
+                const bool ok = cc < nl;
+                const TI* row = in + vb + (long long)(ub + cc) * a.in_su;
+                for (int l = lo + t; l <= hi; l += kNT) {
+                    T val = T(0);
+                    if (ok && l >= a.ld_lo && l <= a.ld_hi) {
+                        double x = ldin<TI>(row + l);
+                        if (a.has_bc) x = bc_terms(x, a.bc, l, ub + cc, v);
+                        val = (T)x;
+                    }
+                    buf[l * PR + cc] = val;
+                }
+            }
+        } else {
+            const bool ok = c < nl;
+            const TI* col = in + vb + (long long)(ub + c) * a.in_su;
+            for (int l = lo + slot; l <= hi; l += kNT / W) {
+                T val = T(0);
+                if (ok && l >= a.ld_lo && l <= a.ld_hi) val = (T)ldin<TI>(col + (long long)l * a.in_sl);
+                buf[l * PR + c] = val;
+            }
+        }
+    }
+    __syncthreads();
+
+    OutSink<T> sink;
+    sink.Rv = buf;
+    sink.PR = PR;
+    sink.c = c;
+    sink.div = 0;
+    sink.exy = 0.0;
+    sink.lam = 0.0;
+    sink.ez = nullptr;
+    sink.dlo = 0;
+    sink.dhi = -1;
+    sink.zero_line = 0;
+    sink.zz_hi = -1;
+    if (a.kind2 >= 0 && a.has_div) {
+        const int i = min(ub + c, a.u0 + a.nu - 1);
+        sink.div = 1;
+        sink.exy = __ldg(a.dv.ex + i) + __ldg(a.dv.ey + v);
+        sink.lam = a.dv.lambda;
+        sink.ez = a.dv.ez;
+        sink.dlo = a.dv.lo;
+        sink.dhi = a.dv.hi;
+        sink.zero_line = a.dv.perturb && i <= a.dv.xz_hi && v <= a.dv.yz_hi;
+        sink.zz_hi = a.dv.zz_hi;
+    }
+    transform_lines<T, M>(a.kind, buf, red, c, slot, tb, sink);
+    if (a.kind2 >= 0) {
+        sink.div = 0;
+        transform_lines<T, M>(a.kind2, buf, red, c, slot, tb, sink);
+    }
+
+    // ---- store the output window ----
+    {
+        const int lo = a.st_lo, hi = a.st_hi;
+        const long long vb = (long long)v * a.out_sv;
+        const double sc = a.use_scale ? a.scale : 1.0;
+        if (CONTIG) {
+            for (int cc = 0; cc < nl; ++cc) {
+                TO* row = out + vb + (long long)(ub + cc) * a.out_su;
+                for (int l = lo + t; l <= hi; l += kNT) row[l] = (TO)((double)buf[l * PR + cc] * sc);
+            }
+        } else if (c < nl) {
+            TO* col = out + vb + (long long)(ub + c) * a.out_su;
+            for (int l = lo + slot; l <= hi; l += kNT / W)
+                col[(long long)l * a.out_sl] = (TO)((double)buf[l * PR + c] * sc);
+        }
+    }
+}
+
+}  // namespace fast
+}  // namespace chz

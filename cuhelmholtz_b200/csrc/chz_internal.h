@@ -51,6 +51,41 @@ struct PassArgs {
     DivArgs dv;
 };
 
+// Boundary-term sum for element (i, j, k) of f, applied in the reference's
+// order: x left, x right, y left, y right, z left, z right.
+__device__ __forceinline__ double bc_terms(double v, const BcArgs& b, int i, int j, int k) {
+    const long long sfy = b.nx + 1;
+    const long long sfz = (long long)(b.nx + 1) * (b.ny + 1);
+    const double* f = b.f;
+    if (i == b.xs) {
+        if (b.xbc == 1 || b.xbc == 2) v -= __ldg(f + k * sfz + j * sfy) * b.dx2;
+        else if (b.xbc == 3 || b.xbc == 4) v += 2 * __ldg(b.bcl + (long long)k * (b.ny + 1) + j) * b.dx;
+    }
+    if (i == b.xe) {
+        if (b.xbc == 1 || b.xbc == 4) v -= __ldg(f + k * sfz + j * sfy + b.nx) * b.dx2;
+        else if (b.xbc == 2 || b.xbc == 3) v -= 2 * __ldg(b.bcr + (long long)k * (b.ny + 1) + j) * b.dx;
+    }
+    if (j == b.ys) {
+        if (b.ybc == 1 || b.ybc == 2) v -= __ldg(f + k * sfz + i) * b.dy2;
+        else if (b.ybc == 3 || b.ybc == 4) v += 2 * __ldg(b.bcb + (long long)k * (b.nx + 1) + i) * b.dy;
+    }
+    if (j == b.ye) {
+        if (b.ybc == 1 || b.ybc == 4) v -= __ldg(f + k * sfz + b.ny * sfy + i) * b.dy2;
+        else if (b.ybc == 2 || b.ybc == 3) v -= 2 * __ldg(b.bct + (long long)k * (b.nx + 1) + i) * b.dy;
+    }
+    if (k == b.zs) {
+        if (b.zbc == 1 || b.zbc == 2) v -= __ldg(f + j * sfy + i) * b.dz2;
+        else if (b.zbc == 3 || b.zbc == 4) v += 2 * __ldg(b.bcf + (long long)j * (b.nx + 1) + i) * b.dz;
+    }
+    if (k == b.ze) {
+        if (b.zbc == 1 || b.zbc == 4) v -= __ldg(f + b.nz * sfz + j * sfy + i) * b.dz2;
+        else if (b.zbc == 2 || b.zbc == 3) v -= 2 * __ldg(b.bce + (long long)j * (b.nx + 1) + i) * b.dz;
+    }
+    return v;
+}
+
+// Register budget: 3 CTAs of 256 threads per SM except with radices 7..13
+// (2 CTAs), whose butterflies hold more values.
 struct LineGeom {
     int N, M, W, log2W, PR;
     size_t buf_elems;   // elements of T per buffer

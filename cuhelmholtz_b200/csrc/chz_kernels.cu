@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "chz_internal.h"
+#include "chz_fast.cuh"
 
 namespace chz {
 
@@ -31,41 +32,6 @@ constexpr int kThreads = 256;
 template <typename TI>
 __device__ __forceinline__ double ld_in(const TI* p) { return (double)__ldg(p); }
 
-// Boundary-term sum for element (i, j, k) of f, applied in the reference's
-// order: x left, x right, y left, y right, z left, z right.
-__device__ __forceinline__ double bc_apply(double v, const BcArgs& b, int i, int j, int k) {
-    const long long sfy = b.nx + 1;
-    const long long sfz = (long long)(b.nx + 1) * (b.ny + 1);
-    const double* f = b.f;
-    if (i == b.xs) {
-        if (b.xbc == 1 || b.xbc == 2) v -= __ldg(f + k * sfz + j * sfy) * b.dx2;
-        else if (b.xbc == 3 || b.xbc == 4) v += 2 * __ldg(b.bcl + (long long)k * (b.ny + 1) + j) * b.dx;
-    }
-    if (i == b.xe) {
-        if (b.xbc == 1 || b.xbc == 4) v -= __ldg(f + k * sfz + j * sfy + b.nx) * b.dx2;
-        else if (b.xbc == 2 || b.xbc == 3) v -= 2 * __ldg(b.bcr + (long long)k * (b.ny + 1) + j) * b.dx;
-    }
-    if (j == b.ys) {
-        if (b.ybc == 1 || b.ybc == 2) v -= __ldg(f + k * sfz + i) * b.dy2;
-        else if (b.ybc == 3 || b.ybc == 4) v += 2 * __ldg(b.bcb + (long long)k * (b.nx + 1) + i) * b.dy;
-    }
-    if (j == b.ye) {
-        if (b.ybc == 1 || b.ybc == 4) v -= __ldg(f + k * sfz + b.ny * sfy + i) * b.dy2;
-        else if (b.ybc == 2 || b.ybc == 3) v -= 2 * __ldg(b.bct + (long long)k * (b.nx + 1) + i) * b.dy;
-    }
-    if (k == b.zs) {
-        if (b.zbc == 1 || b.zbc == 2) v -= __ldg(f + j * sfy + i) * b.dz2;
-        else if (b.zbc == 3 || b.zbc == 4) v += 2 * __ldg(b.bcf + (long long)j * (b.nx + 1) + i) * b.dz;
-    }
-    if (k == b.ze) {
-        if (b.zbc == 1 || b.zbc == 4) v -= __ldg(f + b.nz * sfz + j * sfy + i) * b.dz2;
-        else if (b.zbc == 2 || b.zbc == 3) v -= 2 * __ldg(b.bce + (long long)j * (b.nx + 1) + i) * b.dz;
-    }
-    return v;
-}
-
-// Register budget: 3 CTAs of 256 threads per SM except with radices 7..13
-// (2 CTAs), whose butterflies hold more values.
 template <typename T, typename TI, typename TO, bool CONTIG, int RSET>
 __global__ void __launch_bounds__(kThreads, RSET == kRadixAll ? 2 : 3)
 line_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tb, int buf_elems) {
@@ -99,7 +65,7 @@ line_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tb, int buf_elems) {
                 T val = T(0);
                 if (c < nl && l >= a.ld_lo && l <= a.ld_hi) {
                     double x = ld_in<TI>(in + vbase + (long long)(ub + c) * a.in_su + l);
-                    if (a.has_bc) x = bc_apply(x, a.bc, l, ub + c, v);
+                    if (a.has_bc) x = bc_terms(x, a.bc, l, ub + c, v);
                     val = (T)x;
                 }
                 buf0[l * PR + c] = val;
@@ -231,6 +197,8 @@ __global__ void periodic_fixup(double* f, int nx, int ny, int nz, int px, int py
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
+
+std::atomic<int> g_force_generic{0};
 
 int factor_radices(int M, RadixPlan* rp) {
     int m = M;
@@ -411,9 +379,60 @@ static int launch_typed(const void* in, void* out, const PassArgs& a, const Devi
     return (int)cudaGetLastError();
 }
 
+// Power-of-two half lengths 16..512 use the register-resident kernel.
+bool fast_path_supported(int M) { return M >= 16 && M <= 512 && (M & (M - 1)) == 0; }
+
+int fast_lines_per_cta(int M) { return fast::kNT / (M / fast::kR); }
+
+template <typename T, typename TI, typename TO, bool CONTIG, int M>
+static int launch_fast_m(const void* in, void* out, const PassArgs& a0, const DeviceLineTables& tb,
+                         int nv, cudaStream_t stream, const char* label) {
+    constexpr int W = fast::Cfg<M>::W;
+    PassArgs a = a0;
+    a.log2W = 0;
+    a.PR = fast::Cfg<M>::PR;
+    const int ntiles = (a.nu + W - 1) / W;
+    if (ntiles <= 0 || nv <= 0) return 0;
+    dim3 grid(ntiles, nv);
+    trace_begin(stream, label);
+    fast::fast_line_pass<T, TI, TO, M, CONTIG><<<grid, fast::kNT, 0, stream>>>(
+        static_cast<const TI*>(in), static_cast<TO*>(out), a, to_tables<T>(tb));
+    count_launch();
+    trace_end(stream);
+    return (int)cudaGetLastError();
+}
+
+template <typename T, typename TI, typename TO, bool CONTIG>
+static int launch_fast(const void* in, void* out, const PassArgs& a, const DeviceLineTables& tb, int nv,
+                       cudaStream_t stream, const char* label) {
+    switch (tb.M) {
+        case 16: return launch_fast_m<T, TI, TO, CONTIG, 16>(in, out, a, tb, nv, stream, label);
+        case 32: return launch_fast_m<T, TI, TO, CONTIG, 32>(in, out, a, tb, nv, stream, label);
+        case 64: return launch_fast_m<T, TI, TO, CONTIG, 64>(in, out, a, tb, nv, stream, label);
+        case 128: return launch_fast_m<T, TI, TO, CONTIG, 128>(in, out, a, tb, nv, stream, label);
+        case 256: return launch_fast_m<T, TI, TO, CONTIG, 256>(in, out, a, tb, nv, stream, label);
+        case 512: return launch_fast_m<T, TI, TO, CONTIG, 512>(in, out, a, tb, nv, stream, label);
+        default: return (int)cudaErrorInvalidValue;
+    }
+}
+
 int launch_line_pass(int is_double, int in_type, int out_type, bool contig, const void* in,
                      void* out, const PassArgs& a, const DeviceLineTables& tb, const LineGeom& g,
                      int nv, cudaStream_t stream, const char* label) {
+    if (fast_path_supported(tb.M) && !g_force_generic) {
+#define CHZ_FAST(T, TI, TO)                                                                  \
+    return contig ? launch_fast<T, TI, TO, true>(in, out, a, tb, nv, stream, label)         \
+                  : launch_fast<T, TI, TO, false>(in, out, a, tb, nv, stream, label)
+        if (is_double) {
+            if (in_type == kIoF64 && out_type == kIoF64) CHZ_FAST(double, double, double);
+        } else {
+            if (in_type == kIoF64 && out_type == kIoF32) CHZ_FAST(float, double, float);
+            if (in_type == kIoF32 && out_type == kIoF32) CHZ_FAST(float, float, float);
+            if (in_type == kIoF32 && out_type == kIoF64) CHZ_FAST(float, float, double);
+        }
+#undef CHZ_FAST
+        return (int)cudaErrorInvalidValue;
+    }
 #define CHZ_DISPATCH(T, TI, TO)                                                              \
     return contig ? launch_typed<T, TI, TO, true>(in, out, a, tb, g, nv, stream, label)     \
                   : launch_typed<T, TI, TO, false>(in, out, a, tb, g, nv, stream, label)
@@ -542,6 +561,11 @@ int chz_trace_collect(char* buf, size_t len) {
     }
     return n;
 }
+
+// Selects the kernel family: 0 = register-resident kernels where supported
+// (default), 1 = the generic shared-memory kernel for every length.  Returns
+// the previous setting.
+int chz_set_kernel_family(int generic_only) { return g_force_generic.exchange(generic_only ? 1 : 0); }
 
 // Total kernel launches issued by this library in this process.
 unsigned long long chz_launch_count(void) { return launch_count(); }

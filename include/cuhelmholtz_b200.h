@@ -107,6 +107,12 @@ int chz_release_cached(void);
 int chz_trace_enable(int on);
 int chz_trace_collect(char* buf, size_t len);
 
+/* Kernel family: 0 (default) uses the register-resident line kernels for
+ * lengths N = 32..1024 that are powers of two and the shared-memory mixed-radix
+ * kernel elsewhere; 1 uses the mixed-radix kernel for every length (both are
+ * checked against the same oracle).  Returns the previous setting. */
+int chz_set_kernel_family(int generic_only);
+
 /* Number of kernel launches this library has issued in this process. */
 unsigned long long chz_launch_count(void);
 

@@ -115,6 +115,20 @@ def test_config3_512_manufactured_exact():
     assert err < TOL, err
 
 
+@pytest.mark.parametrize("bcs", [(1, 2, 0), (3, 4, 0), (0, 0, 0), (2, 1, 4), (4, 3, 2), (1, 1, 1), (3, 3, 3)])
+def test_kernel_families_agree(bcs):
+    """Register-resident and generic kernels give the same solve (1e-13)."""
+    p = gen.random_problem(64, 32, 128, *bcs, -2.0, seed=5)
+    a = gpu_solve(p)
+    prev = api.set_kernel_family(True)
+    try:
+        b = gpu_solve(p)
+    finally:
+        api.set_kernel_family(prev)
+    assert rel(a, b) < 1e-13
+    assert rel(a, emulated(p)) < TOL
+
+
 def test_explicit_workspace_matches_cached():
     p = gen.random_problem(32, 24, 40, 2, 0, 4, -5.0, seed=8)
     ws = torch.empty(api.workspace_size(32, 24, 40) // 8 + 32, dtype=torch.float64, device="cuda")

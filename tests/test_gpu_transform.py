@@ -43,7 +43,8 @@ def _check(d, nx, ny, nz, kinds, inplace):
     assert l2 < TOL, (kinds, l2)
 
 
-@pytest.mark.parametrize("inplace,dims", [(True, (8, 8, 8)), (False, (8, 6, 10))])
+@pytest.mark.parametrize("inplace,dims", [(True, (8, 8, 8)), (False, (8, 6, 10)), (True, (32, 32, 32)),
+                                          (False, (64, 32, 128))])
 def test_all_kind_triples_small(inplace, dims):
     nx, ny, nz = dims
     rng = np.random.default_rng(11)
@@ -52,9 +53,18 @@ def test_all_kind_triples_small(inplace, dims):
         _check(d, nx, ny, nz, kinds, inplace)
 
 
-@pytest.mark.parametrize("n", [4, 6, 10, 16, 24, 32, 40, 56, 64, 88, 96, 104, 128, 160, 256])
-def test_every_kind_per_length(n):
-    """Each kind on each axis at one line length (radices 2..13, odd N/2)."""
+@pytest.fixture(params=["default", "generic"])
+def kernel_family(request):
+    prev = api.set_kernel_family(request.param == "generic")
+    yield request.param
+    api.set_kernel_family(prev)
+
+
+@pytest.mark.parametrize("n", [4, 6, 10, 16, 24, 32, 40, 56, 64, 88, 96, 104, 128, 160, 256, 512, 1024])
+def test_every_kind_per_length(n, kernel_family):
+    """Each kind on each axis at one line length (radices 2..13, odd N/2), with
+    the register-resident kernels (N = 32..1024, powers of two) and with the
+    generic kernel for every length."""
     rng = np.random.default_rng(n)
     other = 6
     for kind in range(8):
