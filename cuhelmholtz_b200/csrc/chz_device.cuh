@@ -44,6 +44,20 @@ __device__ __forceinline__ C2<T> ldtw(const C2<T>* p) { return __ldg(p); }
 template <typename T>
 __device__ __forceinline__ T ldr(const T* p) { return __ldg(p); }
 
+// Asynchronous global -> shared copy of one element (cp.async, no register
+// staging, so a thread keeps all its copies in flight).  valid == false
+// writes zero and reads nothing; `src` must still be a mapped address.
+template <int BYTES>
+__device__ __forceinline__ void cp_async_elem(void* smem_dst, const void* src, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    const int n = valid ? BYTES : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(s), "l"(src), "n"(BYTES), "r"(n)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
 // sqrt(1/2), sqrt(3)/2 to 20 significant digits
 #define CHZ_SQRT_HALF 0.70710678118654752440
 #define CHZ_SQRT3_HALF 0.86602540378443864676

@@ -363,31 +363,74 @@ fast_line_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tb) {
         int lo, hi;
         kind_in_window(a.kind, N, lo, hi);
         const long long vb = (long long)v * a.in_sv;
-        if (CONTIG) {
-            for (int cc = 0; cc < W; ++cc) {
-                const bool ok = cc < nl;
-                const TI* row = in + vb + (long long)(ub + cc) * a.in_su;
-                for (int l = lo + t; l <= hi; l += kNT) {
-                    T val = T(0);
-                    if (ok && l >= a.ld_lo && l <= a.ld_hi) {
-                        double x = ldin<TI>(row + l);
-                        if (a.has_bc) x = bc_terms(x, a.bc, l, ub + cc, v);
-                        val = (T)x;
+        if constexpr (sizeof(TI) == sizeof(T)) {
+            // asynchronous copies: every copy of the tile is in flight at once
+            if (CONTIG) {
+                for (int cc = 0; cc < W; ++cc) {
+                    const bool ok = cc < nl;
+                    const TI* row = in + vb + (long long)(ok ? ub + cc : ub) * a.in_su;
+                    for (int l = lo + t; l <= hi; l += kNT) {
+                        const bool valid = ok && l >= a.ld_lo && l <= a.ld_hi;
+                        cp_async_elem<sizeof(T)>(&buf[l * PR + cc], valid ? row + l : in, valid);
                     }
-                    buf[l * PR + cc] = val;
+                }
+            } else {
+                const bool ok = c < nl;
+                const TI* col = in + vb + (long long)(ok ? ub + c : ub) * a.in_su;
+                for (int l = lo + slot; l <= hi; l += kNT / W) {
+                    const bool valid = ok && l >= a.ld_lo && l <= a.ld_hi;
+                    cp_async_elem<sizeof(T)>(&buf[l * PR + c], valid ? col + (long long)l * a.in_sl : in, valid);
                 }
             }
-        } else {
-            const bool ok = c < nl;
-            const TI* col = in + vb + (long long)(ub + c) * a.in_su;
-            for (int l = lo + slot; l <= hi; l += kNT / W) {
-                T val = T(0);
-                if (ok && l >= a.ld_lo && l <= a.ld_hi) val = (T)ldin<TI>(col + (long long)l * a.in_sl);
-                buf[l * PR + c] = val;
+            cp_async_wait_all();
+            __syncthreads();
+            if (CONTIG && a.has_bc) {
+                // boundary terms: every entry of a y/z boundary row, else the
+                // entries at xs and xe (one thread applies all terms of an entry)
+                const BcArgs& b = a.bc;
+                for (int cc = 0; cc < nl; ++cc) {
+                    const int j = ub + cc;
+                    const bool rowb = (j == b.ys || j == b.ye || v == b.zs || v == b.ze);
+                    if (rowb) {
+                        for (int l = a.ld_lo + t; l <= a.ld_hi; l += kNT)
+                            buf[l * PR + cc] = (T)bc_terms((double)buf[l * PR + cc], b, l, j, v);
+                    } else if (t == 0) {
+                        buf[b.xs * PR + cc] = (T)bc_terms((double)buf[b.xs * PR + cc], b, b.xs, j, v);
+                        if (b.xe != b.xs)
+                            buf[b.xe * PR + cc] = (T)bc_terms((double)buf[b.xe * PR + cc], b, b.xe, j, v);
+                    }
+                }
+                __syncthreads();
             }
+        } else {
+            if (CONTIG) {
+                for (int cc = 0; cc < W; ++cc) {
+                    const bool ok = cc < nl;
+                    const TI* row = in + vb + (long long)(ub + cc) * a.in_su;
+#pragma unroll 4
+                    for (int l = lo + t; l <= hi; l += kNT) {
+                        T val = T(0);
+                        if (ok && l >= a.ld_lo && l <= a.ld_hi) {
+                            double x = ldin<TI>(row + l);
+                            if (a.has_bc) x = bc_terms(x, a.bc, l, ub + cc, v);
+                            val = (T)x;
+                        }
+                        buf[l * PR + cc] = val;
+                    }
+                }
+            } else {
+                const bool ok = c < nl;
+                const TI* col = in + vb + (long long)(ub + c) * a.in_su;
+#pragma unroll 4
+                for (int l = lo + slot; l <= hi; l += kNT / W) {
+                    T val = T(0);
+                    if (ok && l >= a.ld_lo && l <= a.ld_hi) val = (T)ldin<TI>(col + (long long)l * a.in_sl);
+                    buf[l * PR + c] = val;
+                }
+            }
+            __syncthreads();
         }
     }
-    __syncthreads();
 
     OutSink<T> sink;
     sink.Rv = buf;

@@ -57,32 +57,66 @@ line_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tb, int buf_elems) {
         kind_in_window(a.kind, N, lo, hi);
         const int len = hi - lo + 1;
         const long long vbase = (long long)v * a.in_sv;
-        if (CONTIG) {
-            const int total = len * W;
-            for (int idx = tid; idx < total; idx += nthr) {
-                const int c = idx / len;
-                const int l = lo + (idx - c * len);
-                T val = T(0);
-                if (c < nl && l >= a.ld_lo && l <= a.ld_hi) {
-                    double x = ld_in<TI>(in + vbase + (long long)(ub + c) * a.in_su + l);
-                    if (a.has_bc) x = bc_terms(x, a.bc, l, ub + c, v);
-                    val = (T)x;
+        if constexpr (sizeof(TI) == sizeof(T)) {
+            if (CONTIG) {
+                const int total = len * W;
+                for (int idx = tid; idx < total; idx += nthr) {
+                    const int c = idx / len;
+                    const int l = lo + (idx - c * len);
+                    const bool valid = c < nl && l >= a.ld_lo && l <= a.ld_hi;
+                    const TI* src = valid ? in + vbase + (long long)(ub + c) * a.in_su + l : in;
+                    cp_async_elem<sizeof(T)>(&buf0[l * PR + c], src, valid);
                 }
-                buf0[l * PR + c] = val;
+            } else {
+                const int total = len << log2W;
+                for (int idx = tid; idx < total; idx += nthr) {
+                    const int c = idx & (W - 1);
+                    const int l = lo + (idx >> log2W);
+                    const bool valid = c < nl && l >= a.ld_lo && l <= a.ld_hi;
+                    const TI* src = valid ? in + vbase + (long long)l * a.in_sl + (ub + c) * a.in_su : in;
+                    cp_async_elem<sizeof(T)>(&buf0[l * PR + c], src, valid);
+                }
+            }
+            cp_async_wait_all();
+            __syncthreads();
+            if (CONTIG && a.has_bc) {
+                const int ln = a.ld_hi - a.ld_lo + 1;
+                const int total = ln * nl;
+                for (int idx = tid; idx < total; idx += nthr) {
+                    const int c = idx / ln;
+                    const int l = a.ld_lo + (idx - c * ln);
+                    buf0[l * PR + c] = (T)bc_terms((double)buf0[l * PR + c], a.bc, l, ub + c, v);
+                }
+                __syncthreads();
             }
         } else {
-            const int total = len << log2W;
-            for (int idx = tid; idx < total; idx += nthr) {
-                const int c = idx & (W - 1);
-                const int l = lo + (idx >> log2W);
-                T val = T(0);
-                if (c < nl && l >= a.ld_lo && l <= a.ld_hi)
-                    val = (T)ld_in<TI>(in + vbase + (long long)l * a.in_sl + (ub + c) * a.in_su);
-                buf0[l * PR + c] = val;
+            if (CONTIG) {
+                const int total = len * W;
+                for (int idx = tid; idx < total; idx += nthr) {
+                    const int c = idx / len;
+                    const int l = lo + (idx - c * len);
+                    T val = T(0);
+                    if (c < nl && l >= a.ld_lo && l <= a.ld_hi) {
+                        double x = ld_in<TI>(in + vbase + (long long)(ub + c) * a.in_su + l);
+                        if (a.has_bc) x = bc_terms(x, a.bc, l, ub + c, v);
+                        val = (T)x;
+                    }
+                    buf0[l * PR + c] = val;
+                }
+            } else {
+                const int total = len << log2W;
+                for (int idx = tid; idx < total; idx += nthr) {
+                    const int c = idx & (W - 1);
+                    const int l = lo + (idx >> log2W);
+                    T val = T(0);
+                    if (c < nl && l >= a.ld_lo && l <= a.ld_hi)
+                        val = (T)ld_in<TI>(in + vbase + (long long)l * a.in_sl + (ub + c) * a.in_su);
+                    buf0[l * PR + c] = val;
+                }
             }
+            __syncthreads();
         }
     }
-    __syncthreads();
 
     T* rin = buf0;
     T* other = buf1;
