@@ -5,6 +5,7 @@ usage: python -m cuhelmholtz_b200._build [--force]
 """
 from __future__ import annotations
 
+import concurrent.futures
 import glob
 import os
 import shutil
@@ -44,21 +45,40 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def _compile(src: str, obj: str) -> str:
+    cmd = [nvcc_path(), *ARCH_FLAGS, *NVCC_FLAGS, "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC,
+           "-c", "-o", obj, src]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"nvcc failed on {src}:\n" + res.stdout + res.stderr)
+    return res.stderr
+
+
 def build_library(force: bool = False, verbose: bool = False) -> str:
+    """Compiles every translation unit (in parallel) and links the shared
+    library; a no-op when the library is newer than all sources."""
     if not force and not _stale():
         return LIBPATH
     os.makedirs(LIBDIR, exist_ok=True)
+    objdir = os.path.join(LIBDIR, "obj")
+    os.makedirs(objdir, exist_ok=True)
+    srcs = sources()
+    objs = [os.path.join(objdir, os.path.basename(s) + ".o") for s in srcs]
+    jobs = max(1, min(len(srcs), os.cpu_count() or 1))
+    logs = []
+    with concurrent.futures.ThreadPoolExecutor(jobs) as ex:
+        for src, log in zip(srcs, ex.map(_compile, srcs, objs)):
+            logs.append(f"== {os.path.basename(src)}\n{log}")
     tmp = LIBPATH + ".tmp"
-    cmd = [nvcc_path(), *ARCH_FLAGS, *NVCC_FLAGS, "-shared", "-I", INCLUDE, "-I", CSRC,
-           "-o", tmp, *sources()]
+    cmd = [nvcc_path(), *ARCH_FLAGS, "-shared", "-o", tmp, *objs]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
+        raise RuntimeError("link failed:\n" + res.stdout + res.stderr)
     if verbose:
-        sys.stderr.write(res.stderr)
+        sys.stderr.write("".join(logs))
     os.replace(tmp, LIBPATH)
     with open(os.path.join(LIBDIR, "ptxas.log"), "w") as fh:
-        fh.write(res.stderr)
+        fh.write("".join(logs))
     return LIBPATH
 
 

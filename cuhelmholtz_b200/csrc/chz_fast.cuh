@@ -1,15 +1,22 @@
 // Register-resident line-pass kernel for power-of-two half lengths
-// M = N/2 in {16, 32, 64, 128, 256, 512}.
+// M = N/2 in {16, 32, 64, 128, 256, 512} (N = 32 .. 1024).
 //
-// Each line is transformed by P = M/16 threads; every thread keeps 16 complex
-// values in registers and performs radix-16 butterflies (radix 2/4/8 for the
-// last factor) between shared-memory exchanges (Stockham order).  The kind's
-// pre step is fused into the first stage's shared-memory reads, the post step
-// reads only the partner values each output needs, and in the fused solver
-// pass the eigenvalue division is applied while the forward post step writes.
-// One shared buffer of (N+2) x (W+1) values holds, in turn, the real input
-// line view, the complex FFT view and the real output view; phases are
-// separated by barriers.
+// * Each line is transformed by P = M/16 threads; every thread keeps 16
+//   complex values in registers and performs radix-16 butterflies (radix
+//   2/4/8 for the last factor) between shared-memory exchanges (Stockham
+//   order).  The kind's pre step is fused into the first stage's reads, the
+//   post step reads only the partner values each output needs, and in the
+//   fused solver pass the eigenvalue division is applied while the forward
+//   post step writes.
+// * The transform kind (and the inverse kind of a fused pass) are template
+//   parameters, so every index, window bound and branch is resolved at
+//   compile time.
+// * CTAs are persistent: each loops over tiles of W lines and prefetches the
+//   next tile with cp.async into a second shared buffer while it transforms
+//   the current one, so HBM reads overlap the shared-memory FFT work.
+// One tile buffer of (N+2) x (W+1) values holds, in turn, the real input view,
+// the complex FFT view and the real output view; phases are separated by
+// barriers.
 #pragma once
 #include "chz_device.cuh"
 #include "chz_internal.h"
@@ -23,14 +30,14 @@ constexpr int kR = 16;    // complex values per thread
 template <int M>
 struct Cfg {
     static constexpr int P = M / kR;      // threads per line
-    static constexpr int W = kNT / P;     // lines per CTA
+    static constexpr int W = kNT / P;     // lines per tile
     static constexpr int N = 2 * M;
     static constexpr int L = N + 2;       // padded line
     static constexpr int PR = W + 1;      // real-view pitch (odd: conflict-free transposed access)
     static constexpr int A16 = (M >= 256) ? 2 : 1;               // radix-16 stages
     static constexpr int R0 = M / (A16 == 2 ? 256 : 16);          // last radix (1 = none)
     static constexpr int NST = A16 + (R0 > 1 ? 1 : 0);
-    static constexpr int BUF = L * PR;     // >= 2*M*W
+    static constexpr int BUF = ((L * PR) + 3) & ~3;   // elements per tile buffer (>= 2*M*W)
     static constexpr int RED = P * W;      // DCT1 odd-sum partials
 };
 
@@ -118,56 +125,60 @@ __device__ __forceinline__ void stage_compute(C2<T>* v, int slot, const C2<T>* _
     }
 }
 
-// Complex value A[n] fed to the FFT, computed from the real view (pre step).
-template <typename T>
-__device__ __forceinline__ C2<T> pre_value(int kind, const T* __restrict__ Rv, int PR, int c, int n,
-                                           int N, int M, const LineTables<T>& tb) {
-    if (kind_is_forward_type(kind)) {
-        return mk<T>(fwd_gather<T>(kind, Rv, PR, c, 2 * n, N, M), fwd_gather<T>(kind, Rv, PR, c, 2 * n + 1, N, M));
+// Complex value A[n] fed to the FFT, from the real view (pre step); the kind
+// is a compile-time constant so the gathers fold to fixed offsets.
+template <typename T, int KIND, int M>
+__device__ __forceinline__ C2<T> pre_value(const T* __restrict__ Rv, int c, int n, const LineTables<T>& tb) {
+    constexpr int N = 2 * M;
+    constexpr int PR = Cfg<M>::PR;
+    if constexpr (KIND == kR2C || KIND == kDCT2 || KIND == kDST2) {
+        return mk<T>(fwd_gather<T>(KIND, Rv, PR, c, 2 * n, N, M), fwd_gather<T>(KIND, Rv, PR, c, 2 * n + 1, N, M));
+    } else {
+        const C2<T> vk = inv_spectrum<T>(KIND, Rv, PR, c, n, N, M, tb);
+        const C2<T> vm = inv_spectrum<T>(KIND, Rv, PR, c, M - n, N, M, tb);
+        const C2<T> wk = ldtw<T>(tb.twN + n);
+        const C2<T> e = cadd<T>(vk, cconj<T>(vm));
+        const C2<T> o = cmul<T>(cconj<T>(wk), csub<T>(vk, cconj<T>(vm)));
+        return cconj<T>(cadd<T>(e, cmul_i<T>(o)));
     }
-    const C2<T> vk = inv_spectrum<T>(kind, Rv, PR, c, n, N, M, tb);
-    const C2<T> vm = inv_spectrum<T>(kind, Rv, PR, c, M - n, N, M, tb);
-    const C2<T> wk = ldtw<T>(tb.twN + n);
-    const C2<T> e = cadd<T>(vk, cconj<T>(vm));
-    const C2<T> o = cmul<T>(cconj<T>(wk), csub<T>(vk, cconj<T>(vm)));
-    return cconj<T>(cadd<T>(e, cmul_i<T>(o)));
 }
 
-// Sink for real outputs of the post step: optional division by the
-// Helmholtz eigenvalue (fused z pass) while writing the real view.
-template <typename T>
+// Sink for real outputs of the post step; with DIV, values on the spectral
+// window are divided by the Helmholtz eigenvalue as they are written.
+template <typename T, int PR, bool DIV>
 struct OutSink {
     T* Rv;
-    int PR, c;
-    int div;          // apply the division
+    int c;
     double exy, lam;  // ex[i] + ey[j], lambda
     const double* ez;
     int dlo, dhi;     // spectral window along the line
-    int zero_line;    // (i, j) is in the zero-mode set; zero entries l <= zz_hi
-    int zz_hi;
+    int zmax;         // entries l <= zmax are zeroed (zero mode), else -1
     __device__ __forceinline__ void put(int l, T val) const {
-        if (div && l >= dlo && l <= dhi) {
-            const double den = (exy + __ldg(ez + l)) + lam;
-            double eig = __drcp_rn(den);
-            if (zero_line && l <= zz_hi) eig = 0.0;
-            val = (T)((double)val * eig);
+        if constexpr (DIV) {
+            if (l >= dlo && l <= dhi) {
+                const double den = (exy + __ldg(ez + l)) + lam;
+                double eig = __drcp_rn(den);
+                if (l <= zmax) eig = 0.0;
+                val = (T)((double)val * eig);
+            }
         }
         Rv[l * PR + c] = val;
     }
 };
 
 // One complete real transform of the W lines held in `buf` (real view in,
-// real view out), for compile-time M and runtime kind.
-template <typename T, int M>
-__device__ __forceinline__ void transform_lines(int kind, T* buf, T* red, int c, int slot,
-                                                const LineTables<T>& tb, const OutSink<T>& sink) {
+// real view out).
+template <typename T, int M, int KIND, typename SINK>
+__device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot, const LineTables<T>& tb,
+                                                const SINK& sink) {
     using CF = Cfg<M>;
     constexpr int W = CF::W, PR = CF::PR, N = CF::N, P = CF::P;
+    constexpr bool FWD = (KIND == kR2C || KIND == kDCT2 || KIND == kDST2);
     C2<T>* Z = reinterpret_cast<C2<T>*>(buf);
     C2<T> v[kR];
 
     // DCT1: partial sums of the odd entries x[1], x[3], ..., x[N-1]
-    if (kind == kDCT1) {
+    if constexpr (KIND == kDCT1) {
         T acc = T(0);
 #pragma unroll
         for (int q = 0; q < M / P; ++q) acc += buf[(2 * (slot + q * P) + 1) * PR + c];
@@ -178,13 +189,12 @@ __device__ __forceinline__ void transform_lines(int kind, T* buf, T* red, int c,
     {
         using BF = Bfly<M, 0>;
 #pragma unroll
-        for (int k = 0; k < kR; ++k) v[k] = pre_value<T>(kind, buf, PR, c, BF::in_idx(slot, 0, k), N, M, tb);
+        for (int k = 0; k < kR; ++k) v[k] = pre_value<T, KIND, M>(buf, c, BF::in_idx(slot, 0, k), tb);
         __syncthreads();
         stage_compute<T, M, 0>(v, slot, tb.twM);
     }
 
-    // ---- middle and last stages ----
-    // Writes the previous stage's results, then reads this stage's inputs.
+    // ---- middle and last stages: write previous results, read this stage's inputs ----
 #define CHZ_STAGE(S)                                                                          \
     if constexpr (CF::NST > S) {                                                              \
         using PB = Bfly<M, S - 1>;                                                            \
@@ -205,7 +215,7 @@ __device__ __forceinline__ void transform_lines(int kind, T* buf, T* red, int c,
 
     // ---- post step ----
     using LB = Bfly<M, CF::NST - 1>;
-    if (kind_is_forward_type(kind) || kind == kDCT1 || kind == kDST1) {
+    if constexpr (FWD || KIND == kDCT1 || KIND == kDST1) {
         // publish Z, then read the partner entries
 #pragma unroll
         for (int b = 0; b < LB::B; ++b)
@@ -213,7 +223,7 @@ __device__ __forceinline__ void transform_lines(int kind, T* buf, T* red, int c,
             for (int k = 0; k < LB::r; ++k) Z[LB::out_idx(slot, b, k) * W + c] = v[b * LB::r + k];
         __syncthreads();
     }
-    if (kind_is_forward_type(kind)) {
+    if constexpr (FWD) {
         // split: V[m] = 1/2 (Z[m] + conj Z[M-m]) - i/2 w^m (Z[m] - conj Z[M-m])
         C2<T> vM = mk<T>(T(0), T(0));
 #pragma unroll
@@ -236,7 +246,7 @@ __device__ __forceinline__ void transform_lines(int kind, T* buf, T* red, int c,
             for (int k = 0; k < LB::r; ++k) {
                 const int m = LB::out_idx(slot, b, k);
                 const C2<T> V = v[b * LB::r + k];
-                if (kind == kR2C) {
+                if constexpr (KIND == kR2C) {
                     sink.put(2 * m, V.x);
                     sink.put(2 * m + 1, m == 0 ? T(0) : V.y);
                     if (m == 0) {
@@ -245,7 +255,7 @@ __device__ __forceinline__ void transform_lines(int kind, T* buf, T* red, int c,
                     }
                 } else {
                     const C2<T> a = cmul<T>(ldtw<T>(tb.tw4N + m), V);
-                    if (kind == kDCT2) {
+                    if constexpr (KIND == kDCT2) {
                         sink.put(m, a.x);
                         if (m > 0) sink.put(N - m, -a.y);
                     } else {  // DST2
@@ -259,13 +269,15 @@ __device__ __forceinline__ void transform_lines(int kind, T* buf, T* red, int c,
                     }
                 }
             }
-    } else if (kind == kDCT1 || kind == kDST1) {
+    } else if constexpr (KIND == kDCT1 || KIND == kDST1) {
         // v[n] = Re conj(Z[n/2]) (n even), Im conj(Z[n/2]) (n odd); pairs (k, N-k)
         T outs[2 * kR];
         T S = T(0);
-        if (kind == kDCT1 && slot == 0) {
+        if constexpr (KIND == kDCT1) {
+            if (slot == 0) {
 #pragma unroll
-            for (int q = 0; q < P; ++q) S += red[q * W + c];
+                for (int q = 0; q < P; ++q) S += red[q * W + c];
+            }
         }
         T extra = T(0);  // out[N] (DCT1, m = 0)
 #pragma unroll
@@ -275,10 +287,9 @@ __device__ __forceinline__ void transform_lines(int kind, T* buf, T* red, int c,
                 const int m = LB::out_idx(slot, b, k);
                 const C2<T> z = v[b * LB::r + k];
                 const T ve = z.x, vo = -z.y;  // v[2m], v[2m+1]
-                // k = 2m
                 T oe;
                 if (m == 0) {
-                    if (kind == kDCT1) {
+                    if constexpr (KIND == kDCT1) {
                         const T h = T(0.5) * ve;
                         oe = h + S;
                         extra = h - S;
@@ -288,15 +299,14 @@ __device__ __forceinline__ void transform_lines(int kind, T* buf, T* red, int c,
                 } else {
                     const T pe = Z[(M - m) * W + c].x;  // v[N-2m]
                     const T is4 = ldr<T>(tb.inv4sin + (2 * m <= M ? 2 * m : N - 2 * m));
-                    if (kind == kDCT1) oe = ((ve + pe) * T(0.5) - (ve - pe) * is4) * T(0.5);
+                    if constexpr (KIND == kDCT1) oe = ((ve + pe) * T(0.5) - (ve - pe) * is4) * T(0.5);
                     else oe = ((ve + pe) * is4 + (ve - pe) * T(0.5)) * T(0.5);
                 }
-                // k = 2m + 1
                 const T po = -Z[(M - m - 1) * W + c].y;  // v[N-2m-1]
                 const int ko = 2 * m + 1;
                 const T is4o = ldr<T>(tb.inv4sin + (ko <= M ? ko : N - ko));
                 T oo;
-                if (kind == kDCT1) oo = ((vo + po) * T(0.5) - (vo - po) * is4o) * T(0.5);
+                if constexpr (KIND == kDCT1) oo = ((vo + po) * T(0.5) - (vo - po) * is4o) * T(0.5);
                 else oo = ((vo + po) * is4o + (vo - po) * T(0.5)) * T(0.5);
                 outs[2 * (b * LB::r + k)] = oe;
                 outs[2 * (b * LB::r + k) + 1] = oo;
@@ -309,11 +319,13 @@ __device__ __forceinline__ void transform_lines(int kind, T* buf, T* red, int c,
                 const int m = LB::out_idx(slot, b, k);
                 sink.put(2 * m, outs[2 * (b * LB::r + k)]);
                 sink.put(2 * m + 1, outs[2 * (b * LB::r + k) + 1]);
-                if (m == 0 && kind == kDCT1) sink.put(N, extra);
+                if constexpr (KIND == kDCT1) {
+                    if (m == 0) sink.put(N, extra);
+                }
             }
     } else {
         // C2R, DCT3, DST3: outputs come straight from the thread's own values
-        __syncthreads();
+        // (every thread passed the barrier after its last shared reads)
 #pragma unroll
         for (int b = 0; b < LB::B; ++b)
 #pragma unroll
@@ -322,10 +334,10 @@ __device__ __forceinline__ void transform_lines(int kind, T* buf, T* red, int c,
                 const C2<T> z = v[b * LB::r + k];
                 const T v0 = z.x, v1 = -z.y;
                 const int e0 = 2 * m, e1 = 2 * m + 1;
-                if (kind == kC2R) {
+                if constexpr (KIND == kC2R) {
                     sink.put(e0, v0);
                     sink.put(e1, v1);
-                } else if (kind == kDCT3) {
+                } else if constexpr (KIND == kDCT3) {
                     sink.put(e0 < M ? 2 * e0 : 2 * (N - 1 - e0) + 1, T(0.5) * v0);
                     sink.put(e1 < M ? 2 * e1 : 2 * (N - 1 - e1) + 1, T(0.5) * v1);
                 } else {  // DST3
@@ -340,142 +352,162 @@ __device__ __forceinline__ void transform_lines(int kind, T* buf, T* red, int c,
     __syncthreads();
 }
 
+template <int KIND, int N>
+struct InWin {
+    static constexpr int lo = (KIND == kDST1 || KIND == kDST2) ? 1 : 0;
+    static constexpr int hi = (KIND == kDST1) ? N - 1
+                            : (KIND == kDST2 || KIND == kDST3 || KIND == kDCT1) ? N
+                            : (KIND == kC2R) ? N + 1 : N - 1;
+};
+
 template <typename TI>
 __device__ __forceinline__ double ldin(const TI* p) { return (double)__ldg(p); }
 
-template <typename T, typename TI, typename TO, int M, bool CONTIG>
-__global__ void __launch_bounds__(kNT, 4)
-fast_line_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tb) {
+// Issues the loads of one tile (cp.async when no conversion is needed) into
+// `buf` and commits them as one group.
+template <typename T, typename TI, int M, bool CONTIG, int KIND>
+__device__ __forceinline__ void load_tile(T* buf, const TI* __restrict__ in, const PassArgs& a, int ub, int nl,
+                                          int v, int t, int c, int slot) {
     using CF = Cfg<M>;
-    constexpr int W = CF::W, PR = CF::PR, N = CF::N;
-    __shared__ __align__(16) T buf[CF::BUF];
-    __shared__ T red[CF::RED];
+    constexpr int W = CF::W, PR = CF::PR, N = CF::N, P = CF::P;
+    constexpr int LO = InWin<KIND, N>::lo, HI = InWin<KIND, N>::hi;
+    const long long vb = (long long)v * a.in_sv;
+    if constexpr (CONTIG) {
+#pragma unroll 1
+        for (int cc = 0; cc < W; ++cc) {
+            const bool ok = cc < nl;
+            const TI* row = in + vb + (long long)(ok ? ub + cc : ub) * a.in_su;
+#pragma unroll
+            for (int l = LO + t; l <= HI; l += kNT) {
+                const bool valid = ok && l >= a.ld_lo && l <= a.ld_hi;
+                if constexpr (sizeof(TI) == sizeof(T)) {
+                    cp_async_elem<sizeof(T)>(&buf[l * PR + cc], valid ? row + l : in, valid);
+                } else {
+                    buf[l * PR + cc] = valid ? (T)ldin<TI>(row + l) : T(0);
+                }
+            }
+        }
+    } else {
+        const bool ok = c < nl;
+        const TI* p = in + vb + (long long)(ok ? ub + c : ub) * a.in_su + (long long)(LO + slot) * a.in_sl;
+        const long long step = (long long)P * a.in_sl;
+#pragma unroll
+        for (int l = LO + slot; l <= HI; l += P) {
+            const bool valid = ok && l >= a.ld_lo && l <= a.ld_hi;
+            if constexpr (sizeof(TI) == sizeof(T)) {
+                cp_async_elem<sizeof(T)>(&buf[l * PR + c], valid ? p : in, valid);
+            } else {
+                buf[l * PR + c] = valid ? (T)ldin<TI>(p) : T(0);
+            }
+            p += step;
+        }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+template <typename T, typename TI, typename TO, int M, bool CONTIG, int KIND, int KIND2>
+__global__ void __launch_bounds__(kNT, 3)
+fast_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tb, int ntx, int ntiles) {
+    using CF = Cfg<M>;
+    constexpr int W = CF::W, PR = CF::PR, P = CF::P, BUF = CF::BUF;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* bufs = reinterpret_cast<T*>(smem_raw);
+    T* red = bufs + 2 * BUF;
 
     const int t = threadIdx.x;
     const int c = t % W;
     const int slot = t / W;
-    const int ub = a.u0 + blockIdx.x * W;
-    const int nl = min(W, a.u0 + a.nu - ub);
-    const int v = a.v0 + blockIdx.y;
 
-    // ---- load the input window ----
+    int tile = blockIdx.x;
+    if (tile >= ntiles) return;
     {
-        int lo, hi;
-        kind_in_window(a.kind, N, lo, hi);
-        const long long vb = (long long)v * a.in_sv;
-        if constexpr (sizeof(TI) == sizeof(T)) {
-            // asynchronous copies: every copy of the tile is in flight at once
-            if (CONTIG) {
-                for (int cc = 0; cc < W; ++cc) {
-                    const bool ok = cc < nl;
-                    const TI* row = in + vb + (long long)(ok ? ub + cc : ub) * a.in_su;
-                    for (int l = lo + t; l <= hi; l += kNT) {
-                        const bool valid = ok && l >= a.ld_lo && l <= a.ld_hi;
-                        cp_async_elem<sizeof(T)>(&buf[l * PR + cc], valid ? row + l : in, valid);
-                    }
-                }
-            } else {
-                const bool ok = c < nl;
-                const TI* col = in + vb + (long long)(ok ? ub + c : ub) * a.in_su;
-                for (int l = lo + slot; l <= hi; l += kNT / W) {
-                    const bool valid = ok && l >= a.ld_lo && l <= a.ld_hi;
-                    cp_async_elem<sizeof(T)>(&buf[l * PR + c], valid ? col + (long long)l * a.in_sl : in, valid);
-                }
-            }
-            cp_async_wait_all();
-            __syncthreads();
-            if (CONTIG && a.has_bc) {
-                // boundary terms: every entry of a y/z boundary row, else the
-                // entries at xs and xe (one thread applies all terms of an entry)
-                const BcArgs& b = a.bc;
-                for (int cc = 0; cc < nl; ++cc) {
-                    const int j = ub + cc;
-                    const bool rowb = (j == b.ys || j == b.ye || v == b.zs || v == b.ze);
-                    if (rowb) {
-                        for (int l = a.ld_lo + t; l <= a.ld_hi; l += kNT)
-                            buf[l * PR + cc] = (T)bc_terms((double)buf[l * PR + cc], b, l, j, v);
-                    } else if (t == 0) {
-                        buf[b.xs * PR + cc] = (T)bc_terms((double)buf[b.xs * PR + cc], b, b.xs, j, v);
-                        if (b.xe != b.xs)
-                            buf[b.xe * PR + cc] = (T)bc_terms((double)buf[b.xe * PR + cc], b, b.xe, j, v);
-                    }
-                }
-                __syncthreads();
-            }
+        const int tx = tile % ntx;
+        const int ub = a.u0 + tx * W;
+        load_tile<T, TI, M, CONTIG, KIND>(bufs, in, a, ub, min(W, a.u0 + a.nu - ub), a.v0 + tile / ntx, t, c,
+                                          slot);
+    }
+    int cur = 0;
+    for (; tile < ntiles; tile += gridDim.x) {
+        const int tx = tile % ntx;
+        const int v = a.v0 + tile / ntx;
+        const int ub = a.u0 + tx * W;
+        const int nl = min(W, a.u0 + a.nu - ub);
+        T* buf = bufs + cur * BUF;
+        // prefetch the next tile into the other buffer, then wait for this one
+        const int nt = tile + gridDim.x;
+        if (nt < ntiles) {
+            const int nub = a.u0 + (nt % ntx) * W;
+            load_tile<T, TI, M, CONTIG, KIND>(bufs + (cur ^ 1) * BUF, in, a, nub, min(W, a.u0 + a.nu - nub),
+                                              a.v0 + nt / ntx, t, c, slot);
+            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
         } else {
-            if (CONTIG) {
-                for (int cc = 0; cc < W; ++cc) {
-                    const bool ok = cc < nl;
-                    const TI* row = in + vb + (long long)(ub + cc) * a.in_su;
-#pragma unroll 4
-                    for (int l = lo + t; l <= hi; l += kNT) {
-                        T val = T(0);
-                        if (ok && l >= a.ld_lo && l <= a.ld_hi) {
-                            double x = ldin<TI>(row + l);
-                            if (a.has_bc) x = bc_terms(x, a.bc, l, ub + cc, v);
-                            val = (T)x;
-                        }
-                        buf[l * PR + cc] = val;
-                    }
-                }
-            } else {
-                const bool ok = c < nl;
-                const TI* col = in + vb + (long long)(ub + c) * a.in_su;
-#pragma unroll 4
-                for (int l = lo + slot; l <= hi; l += kNT / W) {
-                    T val = T(0);
-                    if (ok && l >= a.ld_lo && l <= a.ld_hi) val = (T)ldin<TI>(col + (long long)l * a.in_sl);
-                    buf[l * PR + c] = val;
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        }
+        __syncthreads();
+
+        if (CONTIG && a.has_bc) {
+            // boundary terms: every entry of a y/z boundary row, else the
+            // entries at xs and xe (one thread applies all terms of an entry)
+            const BcArgs& b = a.bc;
+            for (int cc = 0; cc < nl; ++cc) {
+                const int j = ub + cc;
+                const bool rowb = (j == b.ys || j == b.ye || v == b.zs || v == b.ze);
+                if (rowb) {
+                    for (int l = a.ld_lo + t; l <= a.ld_hi; l += kNT)
+                        buf[l * PR + cc] = (T)bc_terms((double)buf[l * PR + cc], b, l, j, v);
+                } else if (t == 0) {
+                    buf[b.xs * PR + cc] = (T)bc_terms((double)buf[b.xs * PR + cc], b, b.xs, j, v);
+                    if (b.xe != b.xs) buf[b.xe * PR + cc] = (T)bc_terms((double)buf[b.xe * PR + cc], b, b.xe, j, v);
                 }
             }
             __syncthreads();
         }
-    }
 
-    OutSink<T> sink;
-    sink.Rv = buf;
-    sink.PR = PR;
-    sink.c = c;
-    sink.div = 0;
-    sink.exy = 0.0;
-    sink.lam = 0.0;
-    sink.ez = nullptr;
-    sink.dlo = 0;
-    sink.dhi = -1;
-    sink.zero_line = 0;
-    sink.zz_hi = -1;
-    if (a.kind2 >= 0 && a.has_div) {
-        const int i = min(ub + c, a.u0 + a.nu - 1);
-        sink.div = 1;
-        sink.exy = __ldg(a.dv.ex + i) + __ldg(a.dv.ey + v);
-        sink.lam = a.dv.lambda;
-        sink.ez = a.dv.ez;
-        sink.dlo = a.dv.lo;
-        sink.dhi = a.dv.hi;
-        sink.zero_line = a.dv.perturb && i <= a.dv.xz_hi && v <= a.dv.yz_hi;
-        sink.zz_hi = a.dv.zz_hi;
-    }
-    transform_lines<T, M>(a.kind, buf, red, c, slot, tb, sink);
-    if (a.kind2 >= 0) {
-        sink.div = 0;
-        transform_lines<T, M>(a.kind2, buf, red, c, slot, tb, sink);
-    }
-
-    // ---- store the output window ----
-    {
-        const int lo = a.st_lo, hi = a.st_hi;
-        const long long vb = (long long)v * a.out_sv;
-        const double sc = a.use_scale ? a.scale : 1.0;
-        if (CONTIG) {
-            for (int cc = 0; cc < nl; ++cc) {
-                TO* row = out + vb + (long long)(ub + cc) * a.out_su;
-                for (int l = lo + t; l <= hi; l += kNT) row[l] = (TO)((double)buf[l * PR + cc] * sc);
-            }
-        } else if (c < nl) {
-            TO* col = out + vb + (long long)(ub + c) * a.out_su;
-            for (int l = lo + slot; l <= hi; l += kNT / W)
-                col[(long long)l * a.out_sl] = (TO)((double)buf[l * PR + c] * sc);
+        if constexpr (KIND2 >= 0) {
+            OutSink<T, PR, true> s1;
+            s1.Rv = buf;
+            s1.c = c;
+            const int i = min(ub + c, a.u0 + a.nu - 1);
+            s1.exy = __ldg(a.dv.ex + i) + __ldg(a.dv.ey + v);
+            s1.lam = a.dv.lambda;
+            s1.ez = a.dv.ez;
+            s1.dlo = a.dv.lo;
+            s1.dhi = a.dv.hi;
+            s1.zmax = (a.dv.perturb && i <= a.dv.xz_hi && v <= a.dv.yz_hi) ? a.dv.zz_hi : -1;
+            transform_lines<T, M, KIND>(buf, red, c, slot, tb, s1);
+            OutSink<T, PR, false> s2;
+            s2.Rv = buf;
+            s2.c = c;
+            transform_lines<T, M, KIND2>(buf, red, c, slot, tb, s2);
+        } else {
+            OutSink<T, PR, false> s;
+            s.Rv = buf;
+            s.c = c;
+            transform_lines<T, M, KIND>(buf, red, c, slot, tb, s);
         }
+
+        // ---- store the output window ----
+        {
+            const int lo = a.st_lo, hi = a.st_hi;
+            const long long vb = (long long)v * a.out_sv;
+            const double sc = a.use_scale ? a.scale : 1.0;
+            if constexpr (CONTIG) {
+#pragma unroll 1
+                for (int cc = 0; cc < nl; ++cc) {
+                    TO* row = out + vb + (long long)(ub + cc) * a.out_su;
+                    for (int l = lo + t; l <= hi; l += kNT) row[l] = (TO)((double)buf[l * PR + cc] * sc);
+                }
+            } else if (c < nl) {
+                TO* p = out + vb + (long long)(ub + c) * a.out_su + (long long)(lo + slot) * a.out_sl;
+                const long long step = (long long)P * a.out_sl;
+                for (int l = lo + slot; l <= hi; l += P) {
+                    *p = (TO)((double)buf[l * PR + c] * sc);
+                    p += step;
+                }
+            }
+        }
+        __syncthreads();
+        cur ^= 1;
     }
 }
 

@@ -1,0 +1,78 @@
+// Launch of the persistent register-resident kernels (included by the
+// per-length translation units chz_fast_m*.cu, which instantiate it).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+
+#include "chz_fast.cuh"
+
+namespace chz {
+namespace fast {
+
+int device_sm_count();
+
+template <typename T, typename TI, typename TO, int M, bool CONTIG, int KIND, int KIND2>
+int launch_one(const void* in, void* out, const PassArgs& a, const LineTables<T>& tb, int nv,
+               cudaStream_t stream, const char* label) {
+    using CF = Cfg<M>;
+    auto kern = fast_pass<T, TI, TO, M, CONTIG, KIND, KIND2>;
+    const size_t smem = (2 * (size_t)CF::BUF + CF::RED) * sizeof(T);
+    // per instantiation: opt in to the dynamic shared memory, ask how many CTAs fit
+    static std::atomic<int> ctas_per_sm{0};
+    int cps = ctas_per_sm.load(std::memory_order_relaxed);
+    if (cps == 0) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cps, kern, kNT, smem);
+        if (e != cudaSuccess) return (int)e;
+        if (cps < 1) cps = 1;
+        ctas_per_sm.store(cps, std::memory_order_relaxed);
+    }
+    const int ntx = (a.nu + CF::W - 1) / CF::W;
+    const long long ntiles = (long long)ntx * nv;
+    if (ntiles <= 0) return 0;
+    const long long cap = (long long)cps * device_sm_count();
+    const int grid = (int)(ntiles < cap ? ntiles : cap);
+    trace_begin(stream, label);
+    kern<<<grid, kNT, smem, stream>>>(static_cast<const TI*>(in), static_cast<TO*>(out), a, tb, ntx, (int)ntiles);
+    count_launch();
+    trace_end(stream);
+    return (int)cudaGetLastError();
+}
+
+template <typename T, typename TI, typename TO, int M>
+int launch_fast_kind(bool contig, int kind, int kind2, const void* in, void* out, const PassArgs& a,
+                     const LineTables<T>& tb, int nv, cudaStream_t stream, const char* label) {
+#define CHZ_ONE(C, K, K2) return launch_one<T, TI, TO, M, C, K, K2>(in, out, a, tb, nv, stream, label)
+#define CHZ_SINGLE(K)                  \
+    case K:                            \
+        if (contig) CHZ_ONE(true, K, -1); \
+        CHZ_ONE(false, K, -1);
+    if (kind2 < 0) {
+        switch (kind) {
+            CHZ_SINGLE(kDCT1)
+            CHZ_SINGLE(kDCT2)
+            CHZ_SINGLE(kDCT3)
+            CHZ_SINGLE(kDST1)
+            CHZ_SINGLE(kDST2)
+            CHZ_SINGLE(kDST3)
+            CHZ_SINGLE(kR2C)
+            CHZ_SINGLE(kC2R)
+            default: return (int)cudaErrorInvalidValue;
+        }
+    }
+    if (contig) return (int)cudaErrorInvalidValue;
+    // fused forward / divide / inverse pairs of the solver's boundary codes
+    if (kind == kR2C && kind2 == kC2R) CHZ_ONE(false, kR2C, kC2R);
+    if (kind == kDST1 && kind2 == kDST1) CHZ_ONE(false, kDST1, kDST1);
+    if (kind == kDST3 && kind2 == kDST2) CHZ_ONE(false, kDST3, kDST2);
+    if (kind == kDCT1 && kind2 == kDCT1) CHZ_ONE(false, kDCT1, kDCT1);
+    if (kind == kDCT3 && kind2 == kDCT2) CHZ_ONE(false, kDCT3, kDCT2);
+#undef CHZ_SINGLE
+#undef CHZ_ONE
+    return (int)cudaErrorInvalidValue;
+}
+
+}  // namespace fast
+}  // namespace chz

@@ -23,7 +23,6 @@
 #include <vector>
 
 #include "chz_internal.h"
-#include "chz_fast.cuh"
 
 namespace chz {
 
@@ -413,39 +412,39 @@ static int launch_typed(const void* in, void* out, const PassArgs& a, const Devi
     return (int)cudaGetLastError();
 }
 
-// Power-of-two half lengths 16..512 use the register-resident kernel.
+// Power-of-two half lengths 16..512 use the register-resident kernels (FP64).
 bool fast_path_supported(int M) { return M >= 16 && M <= 512 && (M & (M - 1)) == 0; }
 
-int fast_lines_per_cta(int M) { return fast::kNT / (M / fast::kR); }
+namespace fast {
+template <typename T, typename TI, typename TO, int M>
+int launch_fast_kind(bool contig, int kind, int kind2, const void* in, void* out, const PassArgs& a,
+                     const LineTables<T>& tb, int nv, cudaStream_t stream, const char* label);
 
-template <typename T, typename TI, typename TO, bool CONTIG, int M>
-static int launch_fast_m(const void* in, void* out, const PassArgs& a0, const DeviceLineTables& tb,
-                         int nv, cudaStream_t stream, const char* label) {
-    constexpr int W = fast::Cfg<M>::W;
-    PassArgs a = a0;
-    a.log2W = 0;
-    a.PR = fast::Cfg<M>::PR;
-    const int ntiles = (a.nu + W - 1) / W;
-    if (ntiles <= 0 || nv <= 0) return 0;
-    dim3 grid(ntiles, nv);
-    trace_begin(stream, label);
-    fast::fast_line_pass<T, TI, TO, M, CONTIG><<<grid, fast::kNT, 0, stream>>>(
-        static_cast<const TI*>(in), static_cast<TO*>(out), a, to_tables<T>(tb));
-    count_launch();
-    trace_end(stream);
-    return (int)cudaGetLastError();
+int device_sm_count() {
+    static std::atomic<int> cached[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    int v = cached[dev].load(std::memory_order_relaxed);
+    if (v == 0) {
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        if (v <= 0) v = 1;
+        cached[dev].store(v, std::memory_order_relaxed);
+    }
+    return v;
 }
+}  // namespace fast
 
-template <typename T, typename TI, typename TO, bool CONTIG>
-static int launch_fast(const void* in, void* out, const PassArgs& a, const DeviceLineTables& tb, int nv,
-                       cudaStream_t stream, const char* label) {
+static int launch_fast(bool contig, const void* in, void* out, const PassArgs& a, const DeviceLineTables& tb,
+                       int nv, cudaStream_t stream, const char* label) {
+    const LineTables<double> t = to_tables<double>(tb);
     switch (tb.M) {
-        case 16: return launch_fast_m<T, TI, TO, CONTIG, 16>(in, out, a, tb, nv, stream, label);
-        case 32: return launch_fast_m<T, TI, TO, CONTIG, 32>(in, out, a, tb, nv, stream, label);
-        case 64: return launch_fast_m<T, TI, TO, CONTIG, 64>(in, out, a, tb, nv, stream, label);
-        case 128: return launch_fast_m<T, TI, TO, CONTIG, 128>(in, out, a, tb, nv, stream, label);
-        case 256: return launch_fast_m<T, TI, TO, CONTIG, 256>(in, out, a, tb, nv, stream, label);
-        case 512: return launch_fast_m<T, TI, TO, CONTIG, 512>(in, out, a, tb, nv, stream, label);
+        case 16: return fast::launch_fast_kind<double, double, double, 16>(contig, a.kind, a.kind2, in, out, a, t, nv, stream, label);
+        case 32: return fast::launch_fast_kind<double, double, double, 32>(contig, a.kind, a.kind2, in, out, a, t, nv, stream, label);
+        case 64: return fast::launch_fast_kind<double, double, double, 64>(contig, a.kind, a.kind2, in, out, a, t, nv, stream, label);
+        case 128: return fast::launch_fast_kind<double, double, double, 128>(contig, a.kind, a.kind2, in, out, a, t, nv, stream, label);
+        case 256: return fast::launch_fast_kind<double, double, double, 256>(contig, a.kind, a.kind2, in, out, a, t, nv, stream, label);
+        case 512: return fast::launch_fast_kind<double, double, double, 512>(contig, a.kind, a.kind2, in, out, a, t, nv, stream, label);
         default: return (int)cudaErrorInvalidValue;
     }
 }
@@ -453,20 +452,8 @@ static int launch_fast(const void* in, void* out, const PassArgs& a, const Devic
 int launch_line_pass(int is_double, int in_type, int out_type, bool contig, const void* in,
                      void* out, const PassArgs& a, const DeviceLineTables& tb, const LineGeom& g,
                      int nv, cudaStream_t stream, const char* label) {
-    if (fast_path_supported(tb.M) && !g_force_generic) {
-#define CHZ_FAST(T, TI, TO)                                                                  \
-    return contig ? launch_fast<T, TI, TO, true>(in, out, a, tb, nv, stream, label)         \
-                  : launch_fast<T, TI, TO, false>(in, out, a, tb, nv, stream, label)
-        if (is_double) {
-            if (in_type == kIoF64 && out_type == kIoF64) CHZ_FAST(double, double, double);
-        } else {
-            if (in_type == kIoF64 && out_type == kIoF32) CHZ_FAST(float, double, float);
-            if (in_type == kIoF32 && out_type == kIoF32) CHZ_FAST(float, float, float);
-            if (in_type == kIoF32 && out_type == kIoF64) CHZ_FAST(float, float, double);
-        }
-#undef CHZ_FAST
-        return (int)cudaErrorInvalidValue;
-    }
+    if (is_double && in_type == kIoF64 && out_type == kIoF64 && fast_path_supported(tb.M) && !g_force_generic)
+        return launch_fast(contig, in, out, a, tb, nv, stream, label);
 #define CHZ_DISPATCH(T, TI, TO)                                                              \
     return contig ? launch_typed<T, TI, TO, true>(in, out, a, tb, g, nv, stream, label)     \
                   : launch_typed<T, TI, TO, false>(in, out, a, tb, g, nv, stream, label)
