@@ -20,7 +20,6 @@
 #include "funcinterface.h"
 
 namespace chz {
-namespace {
 
 thread_local char g_last_error[512] = "";
 
@@ -46,6 +45,8 @@ int check_len(int n, const char* axis) {
         return fail(CHZ_ERROR_UNSUPPORTED_SIZE, "%s size %d: N/2 has a prime factor above 13", axis, n);
     return CHZ_SUCCESS;
 }
+
+namespace {
 
 int current_device() {
     int d = 0;
@@ -157,14 +158,7 @@ int do_transform_common(double* d_data, double* d_out, int nx, int ny, int nz, i
 // Helmholtz solver planning
 // --------------------------------------------------------------------------
 
-struct AxisSolve {
-    int n, bc;
-    int s, e;        // unknown window (cuda_helmholtz_solver.cu:78-103)
-    int sp0, sp1;    // spectral window: unknown window, or 0..N+1 when periodic
-    int kf, ki;      // forward / inverse kinds
-    double d, d2;    // 1/h and 1/h^2 (solver.cu:44-49)
-    double pidiv, shift;
-};
+}  // namespace
 
 int setup_axis(int n, int bc, double lo, double hi, AxisSolve* a) {
     a->n = n;
@@ -191,6 +185,8 @@ int setup_axis(int n, int bc, double lo, double hi, AxisSolve* a) {
         return fail(CHZ_ERROR_INVALID_VALUE, "degenerate domain extent");
     return CHZ_SUCCESS;
 }
+
+namespace {
 
 // Eigenvalue tables (2 cos(mode*pidiv + shift) - 2) * d^2 per padded entry,
 // cached on the device by (n, bc, d2, device).
@@ -231,6 +227,8 @@ int eig_table(const AxisSolve& a, const double** out) {
     return CHZ_SUCCESS;
 }
 
+}  // namespace
+
 // `int ratio = NX/2 * NY/2 * NZ/2`, doubled per periodic axis (solver.cu:211-215)
 double solver_scale(const AxisSolve& x, const AxisSolve& y, const AxisSolve& z) {
     long long r = x.n / 2;
@@ -250,15 +248,14 @@ int check_faces(const AxisSolve& a, const double* lo, const double* hi, const ch
     return CHZ_SUCCESS;
 }
 
-int solve_fp64(const AxisSolve& X, const AxisSolve& Y, const AxisSolve& Z, const double* bcl,
-               const double* bcr, const double* bcb, const double* bct, const double* bcf,
-               const double* bce, double lambda, double* f, double* ws, cudaStream_t s) {
+// The five line passes and the periodic planes of one FP64 solve, with the
+// per-axis tables and the work array given by the caller.
+int run_solve_passes(const AxisSolve& X, const AxisSolve& Y, const AxisSolve& Z, const DeviceLineTables& tx,
+                     const DeviceLineTables& ty, const DeviceLineTables& tz, const double* ex, const double* ey,
+                     const double* ez, const double* bcl, const double* bcr, const double* bcb,
+                     const double* bct, const double* bcf, const double* bce, double lambda, double* f,
+                     double* ws, cudaStream_t s) {
     int rc;
-    DeviceLineTables tx, ty, tz;
-    if ((rc = tables_for(X.n, 1, &tx)) || (rc = tables_for(Y.n, 1, &ty)) || (rc = tables_for(Z.n, 1, &tz)))
-        return rc;
-    const double *ex, *ey, *ez;
-    if ((rc = eig_table(X, &ex)) || (rc = eig_table(Y, &ey)) || (rc = eig_table(Z, &ez))) return rc;
     const int nx = X.n, ny = Y.n, nz = Z.n;
     const long long fy = nx + 1, fz = (long long)(nx + 1) * (ny + 1);
     const long long wy = nx + 2, wz = (long long)(nx + 2) * (ny + 2);
@@ -360,6 +357,20 @@ int solve_fp64(const AxisSolve& X, const AxisSolve& Y, const AxisSolve& Z, const
     rc = launch_periodic_fixup(f, nx, ny, nz, X.bc, Y.bc, Z.bc, s);
     if (rc) return cuda_fail(rc, "periodic planes");
     return CHZ_SUCCESS;
+}
+
+namespace {
+
+int solve_fp64(const AxisSolve& X, const AxisSolve& Y, const AxisSolve& Z, const double* bcl,
+               const double* bcr, const double* bcb, const double* bct, const double* bcf,
+               const double* bce, double lambda, double* f, double* ws, cudaStream_t s) {
+    int rc;
+    DeviceLineTables tx, ty, tz;
+    if ((rc = tables_for(X.n, 1, &tx)) || (rc = tables_for(Y.n, 1, &ty)) || (rc = tables_for(Z.n, 1, &tz)))
+        return rc;
+    const double *ex, *ey, *ez;
+    if ((rc = eig_table(X, &ex)) || (rc = eig_table(Y, &ey)) || (rc = eig_table(Z, &ez))) return rc;
+    return run_solve_passes(X, Y, Z, tx, ty, tz, ex, ey, ez, bcl, bcr, bcb, bct, bcf, bce, lambda, f, ws, s);
 }
 
 // Library-owned workspaces, one grow-only buffer per (device, stream).

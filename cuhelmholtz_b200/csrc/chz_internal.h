@@ -86,6 +86,16 @@ __device__ __forceinline__ double bc_terms(double v, const BcArgs& b, int i, int
 
 // Register budget: 3 CTAs of 256 threads per SM except with radices 7..13
 // (2 CTAs), whose butterflies hold more values.
+// One axis of a Helmholtz solve (cuda_helmholtz_solver.cu:44-172).
+struct AxisSolve {
+    int n, bc;
+    int s, e;        // unknown window (cuda_helmholtz_solver.cu:78-103)
+    int sp0, sp1;    // spectral window: unknown window, or 0..N+1 when periodic
+    int kf, ki;      // forward / inverse kinds
+    double d, d2;    // 1/h and 1/h^2 (solver.cu:44-49)
+    double pidiv, shift;
+};
+
 struct LineGeom {
     int N, M, W, log2W, PR;
     size_t buf_elems;   // elements of T per buffer
@@ -124,5 +134,19 @@ unsigned long long launch_count();
 void count_launch();
 int launch_periodic_fixup(double* f, int nx, int ny, int nz, int xbc, int ybc, int zbc,
                           cudaStream_t stream);
+
+// Host helpers shared by the API translation units (chz_api.cu).
+int fail(int status, const char* fmt, ...);
+int cuda_fail(int err, const char* where);
+int check_len(int n, const char* axis);
+int setup_axis(int n, int bc, double lo, double hi, AxisSolve* a);
+int check_faces(const AxisSolve& a, const double* lo, const double* hi, const char* name);
+double solver_scale(const AxisSolve& x, const AxisSolve& y, const AxisSolve& z);
+int run_solve_passes(const AxisSolve& X, const AxisSolve& Y, const AxisSolve& Z, const DeviceLineTables& tx,
+                     const DeviceLineTables& ty, const DeviceLineTables& tz, const double* ex, const double* ey,
+                     const double* ez, const double* bcl, const double* bcr, const double* bcb,
+                     const double* bct, const double* bcf, const double* bce, double lambda, double* f,
+                     double* ws, cudaStream_t s);
+extern thread_local char g_last_error[512];
 
 }  // namespace chz
