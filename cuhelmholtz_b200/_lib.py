@@ -37,6 +37,10 @@ SIGNATURES = {
                                        c_double, c_double, c_int, c_int, _dp, _dp,
                                        c_double, c_double, c_int, c_int, _dp, _dp,
                                        c_double, _dp, c_void_p, c_size_t, c_void_p]),
+    "chz_helmholtz_solve_noalloc": (c_int, [c_double, c_double, c_int, c_int, _dp, _dp,
+                                            c_double, c_double, c_int, c_int, _dp, _dp,
+                                            c_double, c_double, c_int, c_int, _dp, _dp,
+                                            c_double, _dp, c_void_p]),
     "chz_release_cached": (c_int, []),
     "chz_trace_enable": (c_int, [c_int]),
     "chz_trace_collect": (c_int, [c_char_p, c_size_t]),

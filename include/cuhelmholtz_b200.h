@@ -93,6 +93,25 @@ int chz_helmholtz_solve_ws(double left, double right, int nx, int xbc,
                            double lambda, double* f,
                            void* workspace, size_t workspace_bytes, void* stream);
 
+/* FP64 Helmholtz solve that allocates no device memory (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc -- device memory owned
+ * by another allocator or arena, a hard memory budget, or code that must not
+ * wait on the allocator.  The work array and the per-axis tables are
+ * file-scope __device__ arrays of fixed size (64 MiB + about 108 KiB), held by every
+ * GPU that loads the library until exit.  Limits: (NX+2)(NY+2)(NZ+2) <= 2^23
+ * and at most 1024 cells per axis; larger problems return
+ * CHZ_ERROR_UNSUPPORTED_SIZE.  All calls share the arrays (calls that overlap
+ * on the GPU race); each call rewrites everything it reads.  The first call on
+ * a device looks up the arrays' addresses; make it before any stream capture.
+ * Same arguments and results as chz_helmholtz_solve. */
+int chz_helmholtz_solve_noalloc(double left, double right, int nx, int xbc,
+                                const double* bcl, const double* bcr,
+                                double bottom, double top, int ny, int ybc,
+                                const double* bcb, const double* bct,
+                                double front, double back, int nz, int zbc,
+                                const double* bcf, const double* bce,
+                                double lambda, double* f, void* stream);
+
 /* Releases the library-owned workspaces and cached tables of the current
  * device (after synchronising it). */
 int chz_release_cached(void);
