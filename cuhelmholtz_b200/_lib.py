@@ -37,6 +37,12 @@ SIGNATURES = {
                                        c_double, c_double, c_int, c_int, _dp, _dp,
                                        c_double, c_double, c_int, c_int, _dp, _dp,
                                        c_double, _dp, c_void_p, c_size_t, c_void_p]),
+    "chz_helmholtz_solve_refined": (c_int, [c_double, c_double, c_int, c_int, _dp, _dp,
+                                            c_double, c_double, c_int, c_int, _dp, _dp,
+                                            c_double, c_double, c_int, c_int, _dp, _dp,
+                                            c_double, _dp, c_int, c_double,
+                                            ctypes.POINTER(c_int), ctypes.POINTER(c_double),
+                                            c_void_p, c_size_t, c_void_p]),
     "chz_helmholtz_solve_noalloc": (c_int, [c_double, c_double, c_int, c_int, _dp, _dp,
                                             c_double, c_double, c_int, c_int, _dp, _dp,
                                             c_double, c_double, c_int, c_int, _dp, _dp,

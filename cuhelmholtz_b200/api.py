@@ -120,6 +120,34 @@ def cuda_helmholtz_solver(left, right, NX, xbc, bcl, bcr,
     return 0
 
 
+def helmholtz_solve_refined(left, right, NX, xbc, bcl, bcr,
+                            bottom, top, NY, ybc, bcb, bct,
+                            front, back, NZ, zbc, bcf, bce,
+                            lambda_, f, max_corrections: int = 2, tol: float = 0.0,
+                            stream=None, workspace: Optional[torch.Tensor] = None,
+                            report: bool = False):
+    """FP32 transforms + FP64-residual iterative refinement, in place on
+    ``f``.  Returns (corrections_done, last relative residual or -1)."""
+    import ctypes
+    n = (NX + 1) * (NY + 1) * (NZ + 1)
+    pf = _ptr(f, "f", n)
+    fx, fy, fz = (_face_len(a, NX, NY, NZ) for a in "xyz")
+    faces = [_ptr(bcl, "bcl", fx), _ptr(bcr, "bcr", fx), _ptr(bcb, "bcb", fy),
+             _ptr(bct, "bct", fy), _ptr(bcf, "bcf", fz), _ptr(bce, "bce", fz)]
+    done = ctypes.c_int(0)
+    relr = ctypes.c_double(-1.0)
+    ws = workspace.data_ptr() if workspace is not None else None
+    wsb = workspace.numel() * workspace.element_size() if workspace is not None else 0
+    st = _lib.lib().chz_helmholtz_solve_refined(
+        float(left), float(right), NX, xbc, faces[0], faces[1],
+        float(bottom), float(top), NY, ybc, faces[2], faces[3],
+        float(front), float(back), NZ, zbc, faces[4], faces[5],
+        float(lambda_), pf, int(max_corrections), float(tol),
+        ctypes.byref(done), ctypes.byref(relr) if report else None, ws, wsb, _stream(stream))
+    _check(st)
+    return done.value, relr.value
+
+
 def set_kernel_family(generic_only: bool) -> bool:
     """Selects the register-resident kernels (default) or the generic
     mixed-radix kernel for every length; returns the previous setting."""

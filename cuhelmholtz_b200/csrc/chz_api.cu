@@ -46,8 +46,6 @@ int check_len(int n, const char* axis) {
     return CHZ_SUCCESS;
 }
 
-namespace {
-
 int current_device() {
     int d = 0;
     cudaGetDevice(&d);
@@ -61,6 +59,8 @@ int tables_for(int n, int is_double, DeviceLineTables* t) {
     if (rc != 0) return cuda_fail(rc, "table upload");
     return CHZ_SUCCESS;
 }
+
+namespace {
 
 struct Dims {
     int nx, ny, nz;
@@ -199,6 +199,8 @@ EigCache& eig_cache() {
     return *c;
 }
 
+}  // namespace
+
 int eig_table(const AxisSolve& a, const double** out) {
     EigCache& c = eig_cache();
     unsigned long long bits;
@@ -226,8 +228,6 @@ int eig_table(const AxisSolve& a, const double** out) {
     *out = d;
     return CHZ_SUCCESS;
 }
-
-}  // namespace
 
 // `int ratio = NX/2 * NY/2 * NZ/2`, doubled per periodic axis (solver.cu:211-215)
 double solver_scale(const AxisSolve& x, const AxisSolve& y, const AxisSolve& z) {
@@ -383,6 +383,8 @@ WsCache& ws_cache() {
     return *c;
 }
 
+}  // namespace
+
 int cached_workspace(void* stream, size_t bytes, void** out) {
     WsCache& c = ws_cache();
     std::lock_guard<std::mutex> lk(c.mu);
@@ -404,6 +406,8 @@ int cached_workspace(void* stream, size_t bytes, void** out) {
     *out = slot.first;
     return CHZ_SUCCESS;
 }
+
+namespace {
 
 int solve_common(double left, double right, int nx, int xbc, const double* bcl, const double* bcr,
                  double bottom, double top, int ny, int ybc, const double* bcb, const double* bct,
@@ -470,8 +474,10 @@ size_t chz_helmholtz_workspace_size(int nx, int ny, int nz, int precision) {
     const size_t pe = padded_elems(nx, ny, nz);
     size_t bytes = pe * sizeof(double);
     if (precision == 1) {
-        // FP32 work array + FP64 solution array
-        bytes = pe * sizeof(float) + (size_t)(nx + 1) * (ny + 1) * (nz + 1) * sizeof(double) + 256;
+        // FP32 work array + FP64 solution array + two FP64 norm accumulators,
+        // each piece 256-byte aligned
+        auto r256 = [](size_t b) { return (b + 255) & ~(size_t)255; };
+        bytes = r256(pe * sizeof(float)) + r256((size_t)(nx + 1) * (ny + 1) * (nz + 1) * sizeof(double)) + 256;
     }
     return (bytes + 255) & ~(size_t)255;
 }

@@ -494,15 +494,25 @@ fast_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tb, int ntx, int ntil
             if constexpr (CONTIG) {
 #pragma unroll 1
                 for (int cc = 0; cc < nl; ++cc) {
-                    TO* row = out + vb + (long long)(ub + cc) * a.out_su;
-                    for (int l = lo + t; l <= hi; l += kNT) row[l] = (TO)((double)buf[l * PR + cc] * sc);
+                    const long long ro = vb + (long long)(ub + cc) * a.out_su;
+                    TO* row = out + ro;
+                    if (a.acc) {
+                        const double* arow = a.acc + ro;
+                        for (int l = lo + t; l <= hi; l += kNT) row[l] = (TO)(arow[l] + (double)buf[l * PR + cc] * sc);
+                    } else {
+                        for (int l = lo + t; l <= hi; l += kNT) row[l] = (TO)((double)buf[l * PR + cc] * sc);
+                    }
                 }
             } else if (c < nl) {
-                TO* p = out + vb + (long long)(ub + c) * a.out_su + (long long)(lo + slot) * a.out_sl;
+                const long long o = vb + (long long)(ub + c) * a.out_su + (long long)(lo + slot) * a.out_sl;
+                TO* p = out + o;
+                const double* q = a.acc ? a.acc + o : nullptr;
                 const long long step = (long long)P * a.out_sl;
                 for (int l = lo + slot; l <= hi; l += P) {
-                    *p = (TO)((double)buf[l * PR + c] * sc);
+                    const double x = (double)buf[l * PR + c] * sc;
+                    *p = (TO)(q ? *q + x : x);
                     p += step;
+                    if (q) q += step;
                 }
             }
         }

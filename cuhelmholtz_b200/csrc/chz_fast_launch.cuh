@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <type_traits>
 
 #include "chz_fast.cuh"
 
@@ -41,10 +42,30 @@ int launch_one(const void* in, void* out, const PassArgs& a, const LineTables<T>
     return (int)cudaGetLastError();
 }
 
+// Which (input type, output type, layout, kind) combinations are built: same
+// type everywhere; FP64 -> FP32 only for the first (x, forward) pass of the
+// FP32 solve; FP32 -> FP64 only for its last (x, inverse) pass.
+template <typename T, typename TI, typename TO, bool C, int K, int K2>
+constexpr bool wanted() {
+    constexpr bool same = std::is_same<TI, T>::value && std::is_same<TO, T>::value;
+    constexpr bool fwdk = (K == kR2C || K == kDST1 || K == kDST3 || K == kDCT1 || K == kDCT3);
+    constexpr bool invk = (K == kC2R || K == kDST1 || K == kDST2 || K == kDCT1 || K == kDCT2);
+    if (same) return true;
+    if (std::is_same<TI, double>::value && std::is_same<TO, float>::value) return C && fwdk && K2 < 0;
+    if (std::is_same<TI, float>::value && std::is_same<TO, double>::value) return C && invk && K2 < 0;
+    return false;
+}
+
 template <typename T, typename TI, typename TO, int M>
 int launch_fast_kind(bool contig, int kind, int kind2, const void* in, void* out, const PassArgs& a,
                      const LineTables<T>& tb, int nv, cudaStream_t stream, const char* label) {
-#define CHZ_ONE(C, K, K2) return launch_one<T, TI, TO, M, C, K, K2>(in, out, a, tb, nv, stream, label)
+#define CHZ_ONE(C, K, K2)                                                                   \
+    do {                                                                                    \
+        if constexpr (wanted<T, TI, TO, C, K, K2>())                                        \
+            return launch_one<T, TI, TO, M, C, K, K2>(in, out, a, tb, nv, stream, label);   \
+        else                                                                                \
+            return (int)cudaErrorInvalidValue;                                              \
+    } while (0)
 #define CHZ_SINGLE(K)                  \
     case K:                            \
         if (contig) CHZ_ONE(true, K, -1); \

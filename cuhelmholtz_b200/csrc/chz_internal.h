@@ -43,6 +43,7 @@ struct PassArgs {
     int st_lo, st_hi;  // stored part of the output window
     double scale;
     int use_scale;
+    const double* acc;  // when set: out = acc + scale * value (same indexing as out)
     int PR;       // real-view pitch (>= W)
     int log2W;
     int has_bc;
@@ -148,5 +149,10 @@ int run_solve_passes(const AxisSolve& X, const AxisSolve& Y, const AxisSolve& Z,
                      const double* bct, const double* bcf, const double* bce, double lambda, double* f,
                      double* ws, cudaStream_t s);
 extern thread_local char g_last_error[512];
+int current_device();
+int tables_for(int n, int is_double, DeviceLineTables* t);
+int eig_table(const AxisSolve& a, const double** out);
+int cached_workspace(void* stream, size_t bytes, void** out);
+size_t padded_elems(int nx, int ny, int nz);
 
 }  // namespace chz

@@ -172,7 +172,9 @@ line_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tb, int buf_elems) {
                 if (c < nl) {
                     double x = (double)rout[l * PR + c];
                     if (a.use_scale) x *= sc;
-                    out[vbase + (long long)(ub + c) * a.out_su + l] = (TO)x;
+                    const long long o = vbase + (long long)(ub + c) * a.out_su + l;
+                    if (a.acc) x += a.acc[o];
+                    out[o] = (TO)x;
                 }
             }
         } else {
@@ -183,7 +185,9 @@ line_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tb, int buf_elems) {
                 if (c < nl) {
                     double x = (double)rout[l * PR + c];
                     if (a.use_scale) x *= sc;
-                    out[vbase + (long long)l * a.out_sl + (ub + c) * a.out_su] = (TO)x;
+                    const long long o = vbase + (long long)l * a.out_sl + (ub + c) * a.out_su;
+                    if (a.acc) x += a.acc[o];
+                    out[o] = (TO)x;
                 }
             }
         }
@@ -435,25 +439,41 @@ int device_sm_count() {
 }
 }  // namespace fast
 
-static int launch_fast(bool contig, const void* in, void* out, const PassArgs& a, const DeviceLineTables& tb,
-                       int nv, cudaStream_t stream, const char* label) {
-    const LineTables<double> t = to_tables<double>(tb);
+template <typename T, typename TI, typename TO>
+static int launch_fast_t(bool contig, const void* in, void* out, const PassArgs& a, const DeviceLineTables& tb,
+                         int nv, cudaStream_t stream, const char* label) {
+    const LineTables<T> t = to_tables<T>(tb);
+#define CHZ_M(MM) \
+    case MM: return fast::launch_fast_kind<T, TI, TO, MM>(contig, a.kind, a.kind2, in, out, a, t, nv, stream, label)
     switch (tb.M) {
-        case 16: return fast::launch_fast_kind<double, double, double, 16>(contig, a.kind, a.kind2, in, out, a, t, nv, stream, label);
-        case 32: return fast::launch_fast_kind<double, double, double, 32>(contig, a.kind, a.kind2, in, out, a, t, nv, stream, label);
-        case 64: return fast::launch_fast_kind<double, double, double, 64>(contig, a.kind, a.kind2, in, out, a, t, nv, stream, label);
-        case 128: return fast::launch_fast_kind<double, double, double, 128>(contig, a.kind, a.kind2, in, out, a, t, nv, stream, label);
-        case 256: return fast::launch_fast_kind<double, double, double, 256>(contig, a.kind, a.kind2, in, out, a, t, nv, stream, label);
-        case 512: return fast::launch_fast_kind<double, double, double, 512>(contig, a.kind, a.kind2, in, out, a, t, nv, stream, label);
+        CHZ_M(16);
+        CHZ_M(32);
+        CHZ_M(64);
+        CHZ_M(128);
+        CHZ_M(256);
+        CHZ_M(512);
         default: return (int)cudaErrorInvalidValue;
     }
+#undef CHZ_M
 }
 
 int launch_line_pass(int is_double, int in_type, int out_type, bool contig, const void* in,
                      void* out, const PassArgs& a, const DeviceLineTables& tb, const LineGeom& g,
                      int nv, cudaStream_t stream, const char* label) {
-    if (is_double && in_type == kIoF64 && out_type == kIoF64 && fast_path_supported(tb.M) && !g_force_generic)
-        return launch_fast(contig, in, out, a, tb, nv, stream, label);
+    if (fast_path_supported(tb.M) && !g_force_generic) {
+        if (is_double) {
+            if (in_type == kIoF64 && out_type == kIoF64)
+                return launch_fast_t<double, double, double>(contig, in, out, a, tb, nv, stream, label);
+        } else {
+            if (in_type == kIoF32 && out_type == kIoF32)
+                return launch_fast_t<float, float, float>(contig, in, out, a, tb, nv, stream, label);
+            if (in_type == kIoF64 && out_type == kIoF32)
+                return launch_fast_t<float, double, float>(contig, in, out, a, tb, nv, stream, label);
+            if (in_type == kIoF32 && out_type == kIoF64)
+                return launch_fast_t<float, float, double>(contig, in, out, a, tb, nv, stream, label);
+        }
+        return (int)cudaErrorInvalidValue;
+    }
 #define CHZ_DISPATCH(T, TI, TO)                                                              \
     return contig ? launch_typed<T, TI, TO, true>(in, out, a, tb, g, nv, stream, label)     \
                   : launch_typed<T, TI, TO, false>(in, out, a, tb, g, nv, stream, label)

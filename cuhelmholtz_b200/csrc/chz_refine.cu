@@ -1,0 +1,347 @@
+// FP32 transforms with FP64 iterative refinement: chz_helmholtz_solve_refined.
+//
+// The system is the reference's (cuda_helmholtz_solver.cu:33-380): A u = b on
+// the unknown windows, b = f with the boundary terms of _3d_bc*_ini_*
+// (_cuda_helmholtz_.inl:70-227), A the 7-point operator with homogeneous
+// closures (Dirichlet neighbours 0, Neumann ghost = mirror, periodic wrap).
+//
+//   u0 = S32(b);  repeat: r = b - A u (FP64), c = S32(r), u += c
+//
+// S32 is the five-pass diagonal solve with FP32 transforms (FP64 tables
+// rounded to FP32, eigenvalue division in FP64); r is formed in FP64 and stored
+// as FP32 straight into the work array, which the next correction's first pass
+// transforms in place; the last pass of each correction adds c into the FP64
+// solution u (and the final one writes u + c into f).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "chz_internal.h"
+#include "cuhelmholtz_b200.h"
+
+namespace chz {
+namespace {
+
+struct ResidualArgs {
+    BcArgs bc;                 // b = f + boundary terms
+    const double* u;           // (NZ+1)(NY+1)(NX+1), same layout as f
+    float* r;                  // padded (NZ+2)(NY+2)(NX+2)
+    double lambda;
+    double* sums;              // [0] += r^2, [1] += b^2
+};
+
+// r = b - A u at the unknown nodes, with A's homogeneous closures: Dirichlet
+// neighbours are 0 (their values are in b), a Neumann ghost mirrors the
+// interior neighbour (the flux is in b), periodic neighbours wrap.
+__global__ void residual_kernel(ResidualArgs a) {
+    const BcArgs& b = a.bc;
+    const int i = b.xs + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = b.ys + blockIdx.y;
+    const int k = b.zs + blockIdx.z;
+    double r2 = 0.0, b2 = 0.0;
+    if (i <= b.xe) {
+        const long long sy = b.nx + 1, sz = (long long)(b.nx + 1) * (b.ny + 1);
+        const long long o = k * sz + j * sy + i;
+        const double* u = a.u;
+        const double uc = u[o];
+        // x neighbours
+        double ul, ur;
+        if (i == b.xs) {
+            ul = (b.xbc == 0) ? u[o - i + (b.nx - 1)] : (b.xbc >= 3 ? u[o + 1] : 0.0);
+        } else {
+            ul = u[o - 1];
+        }
+        if (i == b.xe) {
+            ur = (b.xbc == 0) ? u[o - i] : ((b.xbc == 2 || b.xbc == 3) ? u[o - 1] : 0.0);
+        } else {
+            ur = u[o + 1];
+        }
+        double dl, dr;
+        if (j == b.ys) {
+            dl = (b.ybc == 0) ? u[o + (b.ny - 1 - j) * sy] : (b.ybc >= 3 ? u[o + sy] : 0.0);
+        } else {
+            dl = u[o - sy];
+        }
+        if (j == b.ye) {
+            dr = (b.ybc == 0) ? u[o - j * sy] : ((b.ybc == 2 || b.ybc == 3) ? u[o - sy] : 0.0);
+        } else {
+            dr = u[o + sy];
+        }
+        double fl, fr;
+        if (k == b.zs) {
+            fl = (b.zbc == 0) ? u[o + (long long)(b.nz - 1 - k) * sz] : (b.zbc >= 3 ? u[o + sz] : 0.0);
+        } else {
+            fl = u[o - sz];
+        }
+        if (k == b.ze) {
+            fr = (b.zbc == 0) ? u[o - (long long)k * sz] : ((b.zbc == 2 || b.zbc == 3) ? u[o - sz] : 0.0);
+        } else {
+            fr = u[o + sz];
+        }
+        const double au = (((ul - 2.0 * uc + ur) * b.dx2 + (dl - 2.0 * uc + dr) * b.dy2) +
+                           (fl - 2.0 * uc + fr) * b.dz2) + a.lambda * uc;
+        const double bv = bc_terms(__ldg(b.f + o), b, i, j, k);
+        const double rv = bv - au;
+        const long long wy = b.nx + 2, wz = (long long)(b.nx + 2) * (b.ny + 2);
+        a.r[k * wz + j * wy + i] = (float)rv;
+        r2 = rv * rv;
+        b2 = bv * bv;
+    }
+    if (a.sums) {
+        // block reduction, then one atomic per block
+        __shared__ double s0[32], s1[32];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            r2 += __shfl_down_sync(0xffffffffu, r2, off);
+            b2 += __shfl_down_sync(0xffffffffu, b2, off);
+        }
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        if (lane == 0) {
+            s0[wid] = r2;
+            s1[wid] = b2;
+        }
+        __syncthreads();
+        if (wid == 0) {
+            const int nw = blockDim.x >> 5;
+            r2 = lane < nw ? s0[lane] : 0.0;
+            b2 = lane < nw ? s1[lane] : 0.0;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                r2 += __shfl_down_sync(0xffffffffu, r2, off);
+                b2 += __shfl_down_sync(0xffffffffu, b2, off);
+            }
+            if (lane == 0) {
+                atomicAdd(a.sums, r2);
+                atomicAdd(a.sums + 1, b2);
+            }
+        }
+    }
+}
+
+// Copies the solution window of u into f (when refinement stops early).
+__global__ void copy_window(double* f, const double* u, int nx, int ny, int xs, int xe, int ys, int zs) {
+    const int i = xs + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = ys + blockIdx.y;
+    const int k = zs + blockIdx.z;
+    if (i > xe) return;
+    const long long o = (long long)k * (nx + 1) * (ny + 1) + (long long)j * (nx + 1) + i;
+    f[o] = u[o];
+}
+
+// One FP32 diagonal solve: x forward (from `in`: f with boundary terms, or
+// the FP32 residual in the work array), y forward, z forward + divide + z
+// inverse, y inverse, x inverse into `out` (FP64; out = acc + c when acc).
+int solve32_passes(const AxisSolve& X, const AxisSolve& Y, const AxisSolve& Z, const DeviceLineTables& tx,
+                   const DeviceLineTables& ty, const DeviceLineTables& tz, const double* ex, const double* ey,
+                   const double* ez, double lambda, const BcArgs* bc, const double* f_in, float* w,
+                   double* out, const double* acc, cudaStream_t s) {
+    int rc;
+    const int nx = X.n, ny = Y.n, nz = Z.n;
+    const long long fy = nx + 1, fz = (long long)(nx + 1) * (ny + 1);
+    const long long wy = nx + 2, wz = (long long)(nx + 2) * (ny + 2);
+    {
+        const LineGeom g = line_geometry(nx, 0, true);
+        PassArgs a{};
+        a.kind = X.kf; a.kind2 = -1;
+        a.u0 = Y.s; a.nu = Y.e - Y.s + 1; a.v0 = Z.s;
+        if (f_in) {
+            a.in_su = fy; a.in_sv = fz;
+        } else {
+            a.in_su = wy; a.in_sv = wz;
+        }
+        a.in_sl = 1;
+        a.ld_lo = X.s; a.ld_hi = X.e;
+        a.out_su = wy; a.out_sv = wz; a.out_sl = 1;
+        a.st_lo = X.sp0; a.st_hi = X.sp1;
+        a.scale = 1.0; a.use_scale = 0;
+        a.PR = g.PR; a.log2W = g.log2W;
+        if (bc) { a.has_bc = 1; a.bc = *bc; }
+        rc = f_in ? launch_line_pass(0, kIoF64, kIoF32, true, f_in, w, a, tx, g, Z.e - Z.s + 1, s, "refine_x_fwd")
+                  : launch_line_pass(0, kIoF32, kIoF32, true, w, w, a, tx, g, Z.e - Z.s + 1, s, "refine_x_fwd");
+        if (rc) return cuda_fail(rc, "refine pass 1");
+    }
+    {
+        const LineGeom g = line_geometry(ny, 0, false);
+        PassArgs a{};
+        a.kind = Y.kf; a.kind2 = -1;
+        a.u0 = X.sp0; a.nu = X.sp1 - X.sp0 + 1; a.v0 = Z.s;
+        a.in_su = 1; a.in_sv = wz; a.in_sl = wy;
+        a.ld_lo = Y.s; a.ld_hi = Y.e;
+        a.out_su = 1; a.out_sv = wz; a.out_sl = wy;
+        a.st_lo = Y.sp0; a.st_hi = Y.sp1;
+        a.scale = 1.0; a.use_scale = 0;
+        a.PR = g.PR; a.log2W = g.log2W;
+        rc = launch_line_pass(0, kIoF32, kIoF32, false, w, w, a, ty, g, Z.e - Z.s + 1, s, "refine_y_fwd");
+        if (rc) return cuda_fail(rc, "refine pass 2");
+    }
+    {
+        const LineGeom g = line_geometry(nz, 0, false);
+        PassArgs a{};
+        a.kind = Z.kf; a.kind2 = Z.ki;
+        a.u0 = X.sp0; a.nu = X.sp1 - X.sp0 + 1; a.v0 = Y.sp0;
+        a.in_su = 1; a.in_sv = wy; a.in_sl = wz;
+        a.ld_lo = Z.s; a.ld_hi = Z.e;
+        a.out_su = 1; a.out_sv = wy; a.out_sl = wz;
+        a.st_lo = Z.s; a.st_hi = Z.e;
+        a.scale = 1.0; a.use_scale = 0;
+        a.PR = g.PR; a.log2W = g.log2W;
+        a.has_div = 1;
+        a.dv.ex = ex; a.dv.ey = ey; a.dv.ez = ez;
+        a.dv.lambda = lambda;
+        a.dv.perturb = (lambda == 0.0 && (X.bc == 0 || X.bc == 3) && (Y.bc == 0 || Y.bc == 3) &&
+                        (Z.bc == 0 || Z.bc == 3));
+        a.dv.xz_hi = X.bc == 0 ? 1 : 0;
+        a.dv.yz_hi = Y.bc == 0 ? 1 : 0;
+        a.dv.zz_hi = Z.bc == 0 ? 1 : 0;
+        a.dv.lo = Z.sp0; a.dv.hi = Z.sp1;
+        rc = launch_line_pass(0, kIoF32, kIoF32, false, w, w, a, tz, g, Y.sp1 - Y.sp0 + 1, s, "refine_z_fwd_div_inv");
+        if (rc) return cuda_fail(rc, "refine pass 3");
+    }
+    {
+        const LineGeom g = line_geometry(ny, 0, false);
+        PassArgs a{};
+        a.kind = Y.ki; a.kind2 = -1;
+        a.u0 = X.sp0; a.nu = X.sp1 - X.sp0 + 1; a.v0 = Z.s;
+        a.in_su = 1; a.in_sv = wz; a.in_sl = wy;
+        a.ld_lo = Y.sp0; a.ld_hi = Y.sp1;
+        a.out_su = 1; a.out_sv = wz; a.out_sl = wy;
+        a.st_lo = Y.s; a.st_hi = Y.e;
+        a.scale = 1.0; a.use_scale = 0;
+        a.PR = g.PR; a.log2W = g.log2W;
+        rc = launch_line_pass(0, kIoF32, kIoF32, false, w, w, a, ty, g, Z.e - Z.s + 1, s, "refine_y_inv");
+        if (rc) return cuda_fail(rc, "refine pass 4");
+    }
+    {
+        const LineGeom g = line_geometry(nx, 0, true);
+        PassArgs a{};
+        a.kind = X.ki; a.kind2 = -1;
+        a.u0 = Y.s; a.nu = Y.e - Y.s + 1; a.v0 = Z.s;
+        a.in_su = wy; a.in_sv = wz; a.in_sl = 1;
+        a.ld_lo = X.sp0; a.ld_hi = X.sp1;
+        a.out_su = fy; a.out_sv = fz; a.out_sl = 1;
+        a.st_lo = X.s; a.st_hi = X.e;
+        a.scale = solver_scale(X, Y, Z); a.use_scale = 1;
+        a.acc = acc;
+        a.PR = g.PR; a.log2W = g.log2W;
+        rc = launch_line_pass(0, kIoF32, kIoF64, true, w, out, a, tx, g, Z.e - Z.s + 1, s, "refine_x_inv");
+        if (rc) return cuda_fail(rc, "refine pass 5");
+    }
+    return CHZ_SUCCESS;
+}
+
+size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+}  // namespace
+}  // namespace chz
+
+using namespace chz;
+
+extern "C" int chz_helmholtz_solve_refined(double left, double right, int nx, int xbc, const double* bcl,
+                                           const double* bcr, double bottom, double top, int ny, int ybc,
+                                           const double* bcb, const double* bct, double front, double back,
+                                           int nz, int zbc, const double* bcf, const double* bce, double lambda,
+                                           double* f, int max_corrections, double tol, int* corrections_done,
+                                           double* rel_residual, void* workspace, size_t workspace_bytes,
+                                           void* stream) {
+    g_last_error[0] = 0;
+    int rc;
+    AxisSolve X, Y, Z;
+    if ((rc = setup_axis(nx, xbc, left, right, &X)) || (rc = setup_axis(ny, ybc, bottom, top, &Y)) ||
+        (rc = setup_axis(nz, zbc, front, back, &Z)))
+        return rc;
+    if ((rc = check_len(nx, "x")) || (rc = check_len(ny, "y")) || (rc = check_len(nz, "z"))) return rc;
+    if (!f) return fail(CHZ_ERROR_INVALID_VALUE, "f is NULL");
+    if (max_corrections < 0 || max_corrections > 64)
+        return fail(CHZ_ERROR_INVALID_VALUE, "max_corrections must be in 0..64");
+    if ((rc = check_faces(X, bcl, bcr, "x")) || (rc = check_faces(Y, bcb, bct, "y")) ||
+        (rc = check_faces(Z, bcf, bce, "z")))
+        return rc;
+    const size_t need = chz_helmholtz_workspace_size(nx, ny, nz, 1);
+    if (workspace) {
+        if (workspace_bytes < need || (reinterpret_cast<uintptr_t>(workspace) & 255))
+            return fail(CHZ_ERROR_WORKSPACE, "workspace needs %zu bytes, 256-byte aligned", need);
+    } else {
+        if ((rc = cached_workspace(stream, need, &workspace))) return rc;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    char* base = static_cast<char*>(workspace);
+    float* w = reinterpret_cast<float*>(base);
+    const size_t wbytes = round256(padded_elems(nx, ny, nz) * sizeof(float));
+    double* u = reinterpret_cast<double*>(base + wbytes);
+    const size_t ubytes = round256((size_t)(nx + 1) * (ny + 1) * (nz + 1) * sizeof(double));
+    double* sums = reinterpret_cast<double*>(base + wbytes + ubytes);
+
+    DeviceLineTables tx, ty, tz;
+    if ((rc = tables_for(nx, 0, &tx)) || (rc = tables_for(ny, 0, &ty)) || (rc = tables_for(nz, 0, &tz))) return rc;
+    const double *ex, *ey, *ez;
+    if ((rc = eig_table(X, &ex)) || (rc = eig_table(Y, &ey)) || (rc = eig_table(Z, &ez))) return rc;
+
+    BcArgs bc{};
+    bc.xbc = X.bc; bc.ybc = Y.bc; bc.zbc = Z.bc;
+    bc.xs = X.s; bc.xe = X.e; bc.ys = Y.s; bc.ye = Y.e; bc.zs = Z.s; bc.ze = Z.e;
+    bc.nx = nx; bc.ny = ny; bc.nz = nz;
+    bc.dx = X.d; bc.dy = Y.d; bc.dz = Z.d;
+    bc.dx2 = X.d2; bc.dy2 = Y.d2; bc.dz2 = Z.d2;
+    bc.f = f;
+    bc.bcl = bcl; bc.bcr = bcr; bc.bcb = bcb; bc.bct = bct; bc.bcf = bcf; bc.bce = bce;
+
+    const bool track = tol > 0.0 || rel_residual != nullptr;
+    int done = 0;
+    double last_rel = -1.0;
+    // initial FP32 solve: into f directly when there is nothing to refine
+    if (max_corrections == 0) {
+        if ((rc = solve32_passes(X, Y, Z, tx, ty, tz, ex, ey, ez, lambda, &bc, f, w, f, nullptr, s))) return rc;
+    } else {
+        if ((rc = solve32_passes(X, Y, Z, tx, ty, tz, ex, ey, ez, lambda, &bc, f, w, u, nullptr, s))) return rc;
+        const dim3 rblock(128, 1, 1);
+        const dim3 rgrid((X.e - X.s + 1 + 127) / 128, Y.e - Y.s + 1, Z.e - Z.s + 1);
+        double prev = -1.0;
+        bool copied = false;
+        for (int it = 0; it < max_corrections; ++it) {
+            ResidualArgs ra;
+            ra.bc = bc;
+            ra.u = u;
+            ra.r = w;
+            ra.lambda = lambda;
+            ra.sums = track ? sums : nullptr;
+            if (track) {
+                cudaError_t e = cudaMemsetAsync(sums, 0, 2 * sizeof(double), s);
+                if (e != cudaSuccess) return cuda_fail((int)e, "memset");
+            }
+            trace_begin(s, "refine_residual");
+            residual_kernel<<<rgrid, rblock, 0, s>>>(ra);
+            count_launch();
+            trace_end(s);
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) return cuda_fail((int)e, "residual");
+            if (track) {
+                double h[2];
+                e = cudaMemcpyAsync(h, sums, sizeof(h), cudaMemcpyDeviceToHost, s);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+                if (e != cudaSuccess) return cuda_fail((int)e, "residual norm");
+                const double rel = h[1] > 0 ? std::sqrt(h[0] / h[1]) : 0.0;
+                last_rel = rel;
+                // stop: residual small enough, or no longer decreasing
+                if ((tol > 0.0 && rel <= tol) || (prev >= 0.0 && rel > 0.5 * prev)) {
+                    const dim3 cgrid = rgrid;
+                    copy_window<<<cgrid, rblock, 0, s>>>(f, u, nx, ny, X.s, X.e, Y.s, Z.s);
+                    count_launch();
+                    copied = true;
+                    break;
+                }
+                prev = rel;
+            }
+            const bool last = (it == max_corrections - 1);
+            if ((rc = solve32_passes(X, Y, Z, tx, ty, tz, ex, ey, ez, lambda, nullptr, nullptr, w, last ? f : u, u, s)))
+                return rc;
+            ++done;
+        }
+        (void)copied;
+    }
+    rc = launch_periodic_fixup(f, nx, ny, nz, X.bc, Y.bc, Z.bc, s);
+    if (rc) return cuda_fail(rc, "periodic planes");
+    if (corrections_done) *corrections_done = done;
+    if (rel_residual) *rel_residual = last_rel;
+    return CHZ_SUCCESS;
+}

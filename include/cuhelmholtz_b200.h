@@ -93,6 +93,29 @@ int chz_helmholtz_solve_ws(double left, double right, int nx, int xbc,
                            double lambda, double* f,
                            void* workspace, size_t workspace_bytes, void* stream);
 
+/* Helmholtz solve with FP32 transforms and FP64 iterative refinement.
+ * u0 = S32(b); then up to max_corrections times: r = b - A u in FP64 (the
+ * 7-point operator with the boundary terms, as the FP64 solve's system),
+ * u += S32(r).  S32 is the diagonal solve with FP32 transforms.  With
+ * tol > 0 (or rel_residual != NULL) the relative residual ||r|| / ||b|| is
+ * read back before each correction (a stream synchronisation) and refinement
+ * stops when it is <= tol or no longer halves; with tol <= 0 and
+ * rel_residual == NULL exactly max_corrections corrections run with no
+ * synchronisation.  corrections_done / rel_residual (may be NULL) report the
+ * corrections applied and the last residual measured (-1 if none).
+ * workspace: NULL for the library-owned one, else at least
+ * chz_helmholtz_workspace_size(nx, ny, nz, 1) bytes, 256-byte aligned.
+ * No counterpart in the reference (its solver is FP64 only). */
+int chz_helmholtz_solve_refined(double left, double right, int nx, int xbc,
+                                const double* bcl, const double* bcr,
+                                double bottom, double top, int ny, int ybc,
+                                const double* bcb, const double* bct,
+                                double front, double back, int nz, int zbc,
+                                const double* bcf, const double* bce,
+                                double lambda, double* f, int max_corrections, double tol,
+                                int* corrections_done, double* rel_residual,
+                                void* workspace, size_t workspace_bytes, void* stream);
+
 /* FP64 Helmholtz solve that allocates no device memory (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc -- device memory owned
  * by another allocator or arena, a hard memory budget, or code that must not
