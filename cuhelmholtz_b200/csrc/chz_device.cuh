@@ -39,10 +39,12 @@ __device__ __forceinline__ C2<T> cmul_negi(C2<T> a) { return mk<T>(a.y, -a.x); }
 template <typename T>
 __device__ __forceinline__ C2<T> cmul_i(C2<T> a) { return mk<T>(-a.y, a.x); }
 
+// Table reads: plain loads, so the same code reads tables in global memory
+// (generic kernel) or staged in shared memory (register-resident kernels).
 template <typename T>
-__device__ __forceinline__ C2<T> ldtw(const C2<T>* p) { return __ldg(p); }
+__device__ __forceinline__ C2<T> ldtw(const C2<T>* p) { return *p; }
 template <typename T>
-__device__ __forceinline__ T ldr(const T* p) { return __ldg(p); }
+__device__ __forceinline__ T ldr(const T* p) { return *p; }
 
 // Asynchronous global -> shared copy of one element (cp.async, no register
 // staging, so a thread keeps all its copies in flight).  valid == false

@@ -11,9 +11,10 @@
 // * The transform kind (and the inverse kind of a fused pass) are template
 //   parameters, so every index, window bound and branch is resolved at
 //   compile time.
-// * CTAs are persistent: each loops over tiles of W lines and prefetches the
-//   next tile with cp.async into a second shared buffer while it transforms
-//   the current one, so HBM reads overlap the shared-memory FFT work.
+// * CTAs are persistent: each stages its line tables in shared memory once and
+//   loops over tiles of W lines; a tile is loaded with cp.async (every copy in
+//   flight at once) and four CTAs per SM overlap one another's loads, FFT work
+//   and stores.
 // One tile buffer of (N+2) x (W+1) values holds, in turn, the real input view,
 // the complex FFT view and the real output view; phases are separated by
 // barriers.
@@ -156,13 +157,23 @@ struct OutSink {
     __device__ __forceinline__ void put(int l, T val) const {
         if constexpr (DIV) {
             if (l >= dlo && l <= dhi) {
-                const double den = (exy + __ldg(ez + l)) + lam;
-                double eig = __drcp_rn(den);
+                const double den = (exy + ez[l]) + lam;
+                double eig = recip(den);
                 if (l <= zmax) eig = 0.0;
                 val = (T)((double)val * eig);
             }
         }
         Rv[l * PR + c] = val;
+    }
+    // 1/d: single-precision seed refined by two Newton-Raphson steps
+    // r <- r + r (1 - d r), which square the relative error each time
+    // (2^-23 -> 2^-46 -> below double rounding).
+    __device__ static __forceinline__ double recip(double d) {
+        double r = (double)__frcp_rn((float)d);
+        double e = fma(-d, r, 1.0);
+        r = fma(r, e, r);
+        e = fma(-d, r, 1.0);
+        return fma(r, e, r);
     }
 };
 
@@ -405,48 +416,70 @@ __device__ __forceinline__ void load_tile(T* buf, const TI* __restrict__ in, con
     asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
 
-template <typename T, typename TI, typename TO, int M, bool CONTIG, int KIND, int KIND2>
-__global__ void __launch_bounds__(kNT, 3)
-fast_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tb, int ntx, int ntiles) {
+// Shared-memory footprint of one CTA (bytes): tile buffer, DCT1 partials,
+// the line tables and, for the fused pass, the z eigenvalue table.
+template <typename T, int M, bool FUSED>
+struct SmemLayout {
     using CF = Cfg<M>;
-    constexpr int W = CF::W, PR = CF::PR, P = CF::P, BUF = CF::BUF;
+    static constexpr size_t buf = 0;
+    static constexpr size_t red = buf + sizeof(T) * CF::BUF;
+    static constexpr size_t twM = (red + sizeof(T) * CF::RED + 15) & ~size_t(15);
+    static constexpr size_t twN = twM + sizeof(C2<T>) * M;
+    static constexpr size_t tw4N = twN + sizeof(C2<T>) * (M + 1);
+    static constexpr size_t inv4sin = tw4N + sizeof(C2<T>) * (M + 1);
+    static constexpr size_t ez = (inv4sin + sizeof(T) * (M + 1) + 15) & ~size_t(15);
+    static constexpr size_t total = ez + (FUSED ? sizeof(double) * (2 * M + 2) : 0);
+};
+
+template <typename T, typename TI, typename TO, int M, bool CONTIG, int KIND, int KIND2>
+__global__ void __launch_bounds__(kNT, 4)
+fast_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tg, int ntx, int ntiles) {
+    using CF = Cfg<M>;
+    using SL = SmemLayout<T, M, (KIND2 >= 0)>;
+    constexpr int W = CF::W, PR = CF::PR, P = CF::P, N = CF::N;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* bufs = reinterpret_cast<T*>(smem_raw);
-    T* red = bufs + 2 * BUF;
+    T* buf = reinterpret_cast<T*>(smem_raw + SL::buf);
+    T* red = reinterpret_cast<T*>(smem_raw + SL::red);
 
     const int t = threadIdx.x;
     const int c = t % W;
     const int slot = t / W;
+    if ((int)blockIdx.x >= ntiles) return;
 
-    int tile = blockIdx.x;
-    if (tile >= ntiles) return;
+    // stage the line tables in shared memory once (the CTA is persistent)
+    LineTables<T> tb = tg;
     {
-        const int tx = tile % ntx;
-        const int ub = a.u0 + tx * W;
-        load_tile<T, TI, M, CONTIG, KIND>(bufs, in, a, ub, min(W, a.u0 + a.nu - ub), a.v0 + tile / ntx, t, c,
-                                          slot);
+        C2<T>* sM = reinterpret_cast<C2<T>*>(smem_raw + SL::twM);
+        C2<T>* sN = reinterpret_cast<C2<T>*>(smem_raw + SL::twN);
+        C2<T>* s4 = reinterpret_cast<C2<T>*>(smem_raw + SL::tw4N);
+        T* sI = reinterpret_cast<T*>(smem_raw + SL::inv4sin);
+        for (int i = t; i < M; i += kNT) sM[i] = tg.twM[i];
+        for (int i = t; i <= M; i += kNT) {
+            sN[i] = tg.twN[i];
+            s4[i] = tg.tw4N[i];
+            sI[i] = tg.inv4sin[i];
+        }
+        tb.twM = sM;
+        tb.twN = sN;
+        tb.tw4N = s4;
+        tb.inv4sin = sI;
     }
-    int cur = 0;
-    for (; tile < ntiles; tile += gridDim.x) {
+    double* ez_s = reinterpret_cast<double*>(smem_raw + SL::ez);
+    if constexpr (KIND2 >= 0) {
+        for (int i = t; i < N + 2; i += kNT) ez_s[i] = a.dv.ez[i];
+    }
+
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int tx = tile % ntx;
         const int v = a.v0 + tile / ntx;
         const int ub = a.u0 + tx * W;
         const int nl = min(W, a.u0 + a.nu - ub);
-        T* buf = bufs + cur * BUF;
-        // prefetch the next tile into the other buffer, then wait for this one
-        const int nt = tile + gridDim.x;
-        if (nt < ntiles) {
-            const int nub = a.u0 + (nt % ntx) * W;
-            load_tile<T, TI, M, CONTIG, KIND>(bufs + (cur ^ 1) * BUF, in, a, nub, min(W, a.u0 + a.nu - nub),
-                                              a.v0 + nt / ntx, t, c, slot);
-            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-        } else {
-            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-        }
+        load_tile<T, TI, M, CONTIG, KIND>(buf, in, a, ub, nl, v, t, c, slot);
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         __syncthreads();
 
         if (CONTIG && a.has_bc) {
-            // boundary terms: every entry of a y/z boundary row, else the
+            // boundary terms: every entry of a y/z boundary row; elsewhere the
             // entries at xs and xe (one thread applies all terms of an entry)
             const BcArgs& b = a.bc;
             for (int cc = 0; cc < nl; ++cc) {
@@ -455,9 +488,9 @@ fast_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tb, int ntx, int ntil
                 if (rowb) {
                     for (int l = a.ld_lo + t; l <= a.ld_hi; l += kNT)
                         buf[l * PR + cc] = (T)bc_terms((double)buf[l * PR + cc], b, l, j, v);
-                } else if (t == 0) {
-                    buf[b.xs * PR + cc] = (T)bc_terms((double)buf[b.xs * PR + cc], b, b.xs, j, v);
-                    if (b.xe != b.xs) buf[b.xe * PR + cc] = (T)bc_terms((double)buf[b.xe * PR + cc], b, b.xe, j, v);
+                } else if (t == 2 * cc || (t == 2 * cc + 1 && b.xe != b.xs)) {
+                    const int l = (t & 1) ? b.xe : b.xs;
+                    buf[l * PR + cc] = (T)bc_terms((double)buf[l * PR + cc], b, l, j, v);
                 }
             }
             __syncthreads();
@@ -470,7 +503,7 @@ fast_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tb, int ntx, int ntil
             const int i = min(ub + c, a.u0 + a.nu - 1);
             s1.exy = __ldg(a.dv.ex + i) + __ldg(a.dv.ey + v);
             s1.lam = a.dv.lambda;
-            s1.ez = a.dv.ez;
+            s1.ez = ez_s;
             s1.dlo = a.dv.lo;
             s1.dhi = a.dv.hi;
             s1.zmax = (a.dv.perturb && i <= a.dv.xz_hi && v <= a.dv.yz_hi) ? a.dv.zz_hi : -1;
@@ -517,7 +550,6 @@ fast_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tb, int ntx, int ntil
             }
         }
         __syncthreads();
-        cur ^= 1;
     }
 }
 

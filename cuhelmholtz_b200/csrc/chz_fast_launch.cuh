@@ -13,12 +13,12 @@ namespace fast {
 
 int device_sm_count();
 
-template <typename T, typename TI, typename TO, int M, bool CONTIG, int KIND, int KIND2>
+template <typename T, typename TI, typename TO, int M, bool CONTIG, int KIND, int K2>
 int launch_one(const void* in, void* out, const PassArgs& a, const LineTables<T>& tb, int nv,
                cudaStream_t stream, const char* label) {
     using CF = Cfg<M>;
-    auto kern = fast_pass<T, TI, TO, M, CONTIG, KIND, KIND2>;
-    const size_t smem = (2 * (size_t)CF::BUF + CF::RED) * sizeof(T);
+    auto kern = fast_pass<T, TI, TO, M, CONTIG, KIND, K2>;
+    const size_t smem = SmemLayout<T, M, (K2 >= 0)>::total;
     // per instantiation: opt in to the dynamic shared memory, ask how many CTAs fit
     static std::atomic<int> ctas_per_sm{0};
     int cps = ctas_per_sm.load(std::memory_order_relaxed);
