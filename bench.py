@@ -447,6 +447,72 @@ def run_ours(args):
     return 0
 
 
+def run_batch(args):
+    """Batching configuration: `--batch-count` problems (sizes uniform in
+    {32, 48, ..., 192} per axis, codes uniform in 0..4, lambda log-uniform in
+    [-100, -0.01], f ~ U[-1, 1]) solved by one graph replay per step, against a
+    loop of one-at-a-time solves of the same problems."""
+    import numpy as np
+    import torch
+
+    import cuhelmholtz_b200 as chz
+    from cuhelmholtz_b200 import _lib
+    from oracle import gen
+    from oracle.stencil import FACE_KEYS
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    probs = gen.config4_problems(count=args.batch_count, seed=4)
+    npts = sum(p["nx"] * p["ny"] * p["nz"] for p in probs)
+    fs = [torch.from_numpy(np.ascontiguousarray(p["f"]).ravel()).cuda() for p in probs]
+    faces = [{k: (None if p.get(k) is None else torch.from_numpy(np.ascontiguousarray(p[k]).ravel()).cuda())
+              for k in FACE_KEYS} for p in probs]
+    plan = chz.BatchPlan(probs)
+    stream = torch.cuda.current_stream()
+
+    def loop():
+        for p, f, fc in zip(probs, fs, faces):
+            d = p["dom"]
+            chz.cuda_helmholtz_solver(d[0], d[1], p["nx"], p["xbc"], fc["bcl"], fc["bcr"],
+                                      d[2], d[3], p["ny"], p["ybc"], fc["bcb"], fc["bct"],
+                                      d[4], d[5], p["nz"], p["zbc"], fc["bcf"], fc["bce"], p["lam"], f)
+
+    def timed(fn, steps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    l0 = _lib.launch_count()
+    ms = timed(lambda: plan.solve(fs, faces), args.steps)
+    launches = _lib.launch_count() - l0
+    ms_loop = timed(loop, args.steps)
+    value = args.batch_count * args.steps / (ms / 1000.0)
+    loop_value = args.batch_count * args.steps / (ms_loop / 1000.0)
+    line = {
+        "metric": "solves/s (batched FP64 Helmholtz solves)", "value": value, "unit": "solves/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"batch_{args.batch_count}_mixed",
+                   "description": "sizes uniform in {32..192 step 16}^3, codes 0..4, lambda -10^U(-2,2)",
+                   "points_per_step": npts},
+        "hbm_gbs_model": 80.0 * npts * args.steps / (ms / 1000.0) / 1e9,
+        "loop_of_single_solves": {"value": loop_value, "ms_per_step": ms_loop / args.steps},
+        "speedup_vs_loop": value / loop_value,
+        "gpu_launches": int(launches),
+    }
+    plan.close()
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -459,6 +525,8 @@ def main():
     ap.add_argument("--ref-procs", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--check", action="store_true", help="report the residual of the solve")
+    ap.add_argument("--batch-count", type=int, default=0,
+                    help="run the batching configuration with this many problems instead")
     ap.add_argument("--refine-corrections", type=int, default=2,
                     help="also time the FP32 + FP64-refinement solve with this many corrections (-1: skip)")
     args = ap.parse_args()
@@ -466,6 +534,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.batch_count > 0:
+        return run_batch(args)
     return run_ours(args)
 
 

@@ -43,6 +43,12 @@ SIGNATURES = {
                                             c_double, _dp, c_int, c_double,
                                             ctypes.POINTER(c_int), ctypes.POINTER(c_double),
                                             c_void_p, c_size_t, c_void_p]),
+    "chz_batch_plan_create": (c_int, [c_int, ctypes.POINTER(c_int), ctypes.POINTER(c_int),
+                                      ctypes.POINTER(c_double), ctypes.POINTER(c_double),
+                                      ctypes.POINTER(c_void_p)]),
+    "chz_batch_solve": (c_int, [c_void_p, ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p), c_void_p]),
+    "chz_batch_workspace_bytes": (c_size_t, [c_void_p]),
+    "chz_batch_plan_destroy": (c_int, [c_void_p]),
     "chz_helmholtz_solve_noalloc": (c_int, [c_double, c_double, c_int, c_int, _dp, _dp,
                                             c_double, c_double, c_int, c_int, _dp, _dp,
                                             c_double, c_double, c_int, c_int, _dp, _dp,

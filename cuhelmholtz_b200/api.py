@@ -148,6 +148,58 @@ def helmholtz_solve_refined(left, right, NX, xbc, bcl, bcr,
     return done.value, relr.value
 
 
+class BatchPlan:
+    """Plan for many independent FP64 solves (sizes, codes, domains, lambdas
+    fixed at creation); ``solve`` runs the whole batch as one graph replay.
+
+    problems: sequence of dicts with keys nx, ny, nz, xbc, ybc, zbc, lam and
+    optionally dom (left, right, bottom, top, front, back)."""
+
+    def __init__(self, problems):
+        import ctypes
+        n = len(problems)
+        self.count = n
+        self.problems = list(problems)
+        dims = (ctypes.c_int * (3 * n))(*[v for p in problems for v in (p["nx"], p["ny"], p["nz"])])
+        bcs = (ctypes.c_int * (3 * n))(*[v for p in problems for v in (p["xbc"], p["ybc"], p["zbc"])])
+        doms = (ctypes.c_double * (6 * n))(*[float(v) for p in problems
+                                             for v in p.get("dom", (0, 1, 0, 1, 0, 1))])
+        lams = (ctypes.c_double * n)(*[float(p["lam"]) for p in problems])
+        self._handle = ctypes.c_void_p()
+        _check(_lib.lib().chz_batch_plan_create(n, dims, bcs, doms, lams, ctypes.byref(self._handle)))
+
+    def solve(self, fs, faces=None, stream=None):
+        """fs: list of CUDA float64 tensors (solved in place); faces: list of
+        dicts {bcl..bce: tensor or None} or None."""
+        import ctypes
+        n = self.count
+        if len(fs) != n:
+            raise ValueError(f"expected {n} right-hand sides")
+        fp = (ctypes.c_void_p * n)(*[_ptr(f, "f", (p["nx"] + 1) * (p["ny"] + 1) * (p["nz"] + 1))
+                                     for f, p in zip(fs, self.problems)])
+        keys = ("bcl", "bcr", "bcb", "bct", "bcf", "bce")
+        if faces is None:
+            fc = None
+        else:
+            fc = (ctypes.c_void_p * (6 * n))(*[(_ptr(d.get(k), k) or None) if d else None
+                                               for d in faces for k in keys])
+        _check(_lib.lib().chz_batch_solve(self._handle, fp, fc, _stream(stream)))
+
+    def workspace_bytes(self) -> int:
+        return int(_lib.lib().chz_batch_workspace_bytes(self._handle))
+
+    def close(self):
+        if self._handle:
+            _lib.lib().chz_batch_plan_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def set_kernel_family(generic_only: bool) -> bool:
     """Selects the register-resident kernels (default) or the generic
     mixed-radix kernel for every length; returns the previous setting."""

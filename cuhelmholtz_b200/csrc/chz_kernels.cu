@@ -24,174 +24,15 @@
 
 #include "chz_internal.h"
 
+#include "chz_generic.cuh"
+
 namespace chz {
-
-constexpr int kThreads = 256;
-
-template <typename TI>
-__device__ __forceinline__ double ld_in(const TI* p) { return (double)__ldg(p); }
 
 template <typename T, typename TI, typename TO, bool CONTIG, int RSET>
 __global__ void __launch_bounds__(kThreads, RSET == kRadixAll ? 2 : 3)
 line_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tb, int buf_elems) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* buf0 = reinterpret_cast<T*>(smem_raw);
-    T* buf1 = buf0 + buf_elems;
-    T* red = buf1 + buf_elems;
-    T* odd = red + kThreads;
-
-    const int tid = threadIdx.x;
-    const int nthr = blockDim.x;
-    const int log2W = a.log2W;
-    const int W = 1 << log2W;
-    const int PR = a.PR;
-    const int N = tb.N;
-    const int ub = a.u0 + blockIdx.x * W;
-    const int nl = min(W, a.u0 + a.nu - ub);
-    const int v = a.v0 + blockIdx.y;
-
-    // ---- load the input window of W lines into buf0 (real view) ----
-    {
-        int lo, hi;
-        kind_in_window(a.kind, N, lo, hi);
-        const int len = hi - lo + 1;
-        const long long vbase = (long long)v * a.in_sv;
-        if constexpr (sizeof(TI) == sizeof(T)) {
-            if (CONTIG) {
-                const int total = len * W;
-                for (int idx = tid; idx < total; idx += nthr) {
-                    const int c = idx / len;
-                    const int l = lo + (idx - c * len);
-                    const bool valid = c < nl && l >= a.ld_lo && l <= a.ld_hi;
-                    const TI* src = valid ? in + vbase + (long long)(ub + c) * a.in_su + l : in;
-                    cp_async_elem<sizeof(T)>(&buf0[l * PR + c], src, valid);
-                }
-            } else {
-                const int total = len << log2W;
-                for (int idx = tid; idx < total; idx += nthr) {
-                    const int c = idx & (W - 1);
-                    const int l = lo + (idx >> log2W);
-                    const bool valid = c < nl && l >= a.ld_lo && l <= a.ld_hi;
-                    const TI* src = valid ? in + vbase + (long long)l * a.in_sl + (ub + c) * a.in_su : in;
-                    cp_async_elem<sizeof(T)>(&buf0[l * PR + c], src, valid);
-                }
-            }
-            cp_async_wait_all();
-            __syncthreads();
-            if (CONTIG && a.has_bc) {
-                const int ln = a.ld_hi - a.ld_lo + 1;
-                const int total = ln * nl;
-                for (int idx = tid; idx < total; idx += nthr) {
-                    const int c = idx / ln;
-                    const int l = a.ld_lo + (idx - c * ln);
-                    buf0[l * PR + c] = (T)bc_terms((double)buf0[l * PR + c], a.bc, l, ub + c, v);
-                }
-                __syncthreads();
-            }
-        } else {
-            if (CONTIG) {
-                const int total = len * W;
-                for (int idx = tid; idx < total; idx += nthr) {
-                    const int c = idx / len;
-                    const int l = lo + (idx - c * len);
-                    T val = T(0);
-                    if (c < nl && l >= a.ld_lo && l <= a.ld_hi) {
-                        double x = ld_in<TI>(in + vbase + (long long)(ub + c) * a.in_su + l);
-                        if (a.has_bc) x = bc_terms(x, a.bc, l, ub + c, v);
-                        val = (T)x;
-                    }
-                    buf0[l * PR + c] = val;
-                }
-            } else {
-                const int total = len << log2W;
-                for (int idx = tid; idx < total; idx += nthr) {
-                    const int c = idx & (W - 1);
-                    const int l = lo + (idx >> log2W);
-                    T val = T(0);
-                    if (c < nl && l >= a.ld_lo && l <= a.ld_hi)
-                        val = (T)ld_in<TI>(in + vbase + (long long)l * a.in_sl + (ub + c) * a.in_su);
-                    buf0[l * PR + c] = val;
-                }
-            }
-            __syncthreads();
-        }
-    }
-
-    T* rin = buf0;
-    T* other = buf1;
-    T* rout = nullptr;
-    int kind = a.kind;
-    const int reps = (a.kind2 >= 0) ? 2 : 1;
-    for (int rep = 0; rep < reps; ++rep) {
-        if (kind == kDCT1) odd_sums<T>(rin, PR, log2W, N, red, odd, tid, nthr);
-        pre_step<T>(kind, rin, PR, reinterpret_cast<C2<T>*>(other), log2W, tb, tid, nthr);
-        __syncthreads();
-        const int res = fft_run<T, RSET>(reinterpret_cast<C2<T>*>(other), reinterpret_cast<C2<T>*>(rin),
-                                   tb.M, log2W, tb.rp, tb.twM, tid, nthr);
-        C2<T>* zres = reinterpret_cast<C2<T>*>(res == 0 ? other : rin);
-        rout = (res == 0) ? rin : other;
-        post_step<T>(kind, zres, rout, PR, log2W, tb, odd, tid, nthr);
-        __syncthreads();
-        if (rep == 0 && a.kind2 >= 0) {
-            if (a.has_div) {
-                const DivArgs& d = a.dv;
-                const int len = d.hi - d.lo + 1;
-                const int total = len << log2W;
-                for (int idx = tid; idx < total; idx += nthr) {
-                    const int c = idx & (W - 1);
-                    const int l = d.lo + (idx >> log2W);
-                    if (c >= nl) continue;
-                    const int i = ub + c;  // x entry (u)
-                    const int j = v;       // y entry (v)
-                    const double den = ((__ldg(d.ex + i) + __ldg(d.ey + j)) + __ldg(d.ez + l)) + d.lambda;
-                    double eig = 1.0 / den;
-                    if (d.perturb && i <= d.xz_hi && j <= d.yz_hi && l <= d.zz_hi) eig = 0.0;
-                    T& r = rout[l * PR + c];
-                    r = (T)((double)r * eig);
-                }
-                __syncthreads();
-            }
-            kind = a.kind2;
-            T* nb = (rout == buf0) ? buf1 : buf0;
-            rin = rout;
-            other = nb;
-        }
-    }
-
-    // ---- store the output window ----
-    {
-        const int lo = a.st_lo, hi = a.st_hi;
-        const int len = hi - lo + 1;
-        const long long vbase = (long long)v * a.out_sv;
-        const double sc = a.scale;
-        if (CONTIG) {
-            const int total = len * W;
-            for (int idx = tid; idx < total; idx += nthr) {
-                const int c = idx / len;
-                const int l = lo + (idx - c * len);
-                if (c < nl) {
-                    double x = (double)rout[l * PR + c];
-                    if (a.use_scale) x *= sc;
-                    const long long o = vbase + (long long)(ub + c) * a.out_su + l;
-                    if (a.acc) x += a.acc[o];
-                    out[o] = (TO)x;
-                }
-            }
-        } else {
-            const int total = len << log2W;
-            for (int idx = tid; idx < total; idx += nthr) {
-                const int c = idx & (W - 1);
-                const int l = lo + (idx >> log2W);
-                if (c < nl) {
-                    double x = (double)rout[l * PR + c];
-                    if (a.use_scale) x *= sc;
-                    const long long o = vbase + (long long)l * a.out_sl + (ub + c) * a.out_su;
-                    if (a.acc) x += a.acc[o];
-                    out[o] = (TO)x;
-                }
-            }
-        }
-    }
+    line_pass_tile<T, TI, TO, CONTIG, RSET>(in, out, a, tb, buf_elems, blockIdx.x, blockIdx.y, smem_raw);
 }
 
 // Periodic planes: every node with index N on a periodic axis takes the value

@@ -93,6 +93,30 @@ int chz_helmholtz_solve_ws(double left, double right, int nx, int xbc,
                            double lambda, double* f,
                            void* workspace, size_t workspace_bytes, void* stream);
 
+/* Batched FP64 solves: `count` independent problems of any supported sizes,
+ * boundary codes, domains and lambdas (no counterpart in the reference, which
+ * solves one problem per call).  The plan precomputes every problem's pass
+ * descriptors and a work array for all of them; each chz_batch_solve runs
+ * the whole batch as six launches (five line passes over the tiles of all
+ * problems, then the periodic planes), captured once into a CUDA graph and
+ * replayed on `stream`.
+ *   dims    : 3*count cell counts (nx, ny, nz per problem)
+ *   bcs     : 3*count boundary codes 0..4
+ *   domains : 6*count extents (left, right, bottom, top, front, back), or
+ *             NULL for the unit cube
+ *   lambdas : count values
+ * chz_batch_solve takes count device pointers f[i] (solved in place, layout
+ * as chz_helmholtz_solve) and 6*count face pointers (bcl, bcr, bcb, bct, bcf,
+ * bce per problem; NULL entries where unused; faces == NULL if none are
+ * used).  It synchronises `stream` once to upload the pointers, then returns
+ * with the graph enqueued. */
+typedef struct chz_batch_plan chz_batch_plan;
+int chz_batch_plan_create(int count, const int* dims, const int* bcs, const double* domains,
+                          const double* lambdas, chz_batch_plan** plan);
+int chz_batch_solve(chz_batch_plan* plan, double* const* f, const double* const* faces, void* stream);
+size_t chz_batch_workspace_bytes(const chz_batch_plan* plan);
+int chz_batch_plan_destroy(chz_batch_plan* plan);
+
 /* Helmholtz solve with FP32 transforms and FP64 iterative refinement.
  * u0 = S32(b); then up to max_corrections times: r = b - A u in FP64 (the
  * 7-point operator with the boundary terms, as the FP64 solve's system),

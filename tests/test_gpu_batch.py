@@ -1,0 +1,85 @@
+"""GPU tests of the batched solver (chz_batch_plan_create / chz_batch_solve):
+many problems of uneven sizes, boundary codes and lambdas in one graph replay
+of six launches, checked against one-at-a-time solves and the oracle."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import emulation as E
+from oracle import gen, stencil
+from cuhelmholtz_b200 import api
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(p):
+    f = torch.from_numpy(np.ascontiguousarray(p["f"]).ravel()).cuda()
+    faces = {k: (None if p.get(k) is None else torch.from_numpy(np.ascontiguousarray(p[k]).ravel()).cuda())
+             for k in stencil.FACE_KEYS}
+    return f, faces
+
+
+def _single(p):
+    f, faces = _dev(p)
+    d = p["dom"]
+    api.cuda_helmholtz_solver(d[0], d[1], p["nx"], p["xbc"], faces["bcl"], faces["bcr"],
+                              d[2], d[3], p["ny"], p["ybc"], faces["bcb"], faces["bct"],
+                              d[4], d[5], p["nz"], p["zbc"], faces["bcf"], faces["bce"], p["lam"], f)
+    torch.cuda.synchronize()
+    return f.cpu().numpy()
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def test_batch_matches_single_solves_and_oracle():
+    probs = gen.config4_problems(count=24, seed=9)
+    plan = api.BatchPlan(probs)
+    devs = [_dev(p) for p in probs]
+    plan.solve([d[0] for d in devs], [d[1] for d in devs])
+    torch.cuda.synchronize()
+    for i, p in enumerate(probs):
+        got = devs[i][0].cpu().numpy()
+        assert _rel(got, _single(p)) < 1e-13, i
+        if i < 4:
+            d = p["dom"]
+            ref = E.emulate_solver(d[0], d[1], p["nx"], p["xbc"], p["bcl"], p["bcr"], d[2], d[3], p["ny"],
+                                   p["ybc"], p["bcb"], p["bct"], d[4], d[5], p["nz"], p["zbc"], p["bcf"],
+                                   p["bce"], p["lam"], p["f"])
+            assert _rel(got.reshape(ref.shape), ref) < 1e-12, i
+    plan.close()
+
+
+def test_batch_graph_replay_with_new_arrays():
+    probs = [gen.random_problem(32, 48, 64, 1, 3, 0, -2.0, seed=1),
+             gen.random_problem(64, 32, 48, 0, 2, 4, -0.3, seed=2),
+             gen.random_problem(48, 48, 48, 3, 3, 3, -9.0, seed=3)]
+    plan = api.BatchPlan(probs)
+    for rep in range(2):
+        devs = [_dev(p) for p in probs]
+        plan.solve([d[0] for d in devs], [d[1] for d in devs])
+        torch.cuda.synchronize()
+        for i, p in enumerate(probs):
+            assert _rel(devs[i][0].cpu().numpy(), _single(p)) < 1e-13, (rep, i)
+    plan.close()
+
+
+def test_config4_512_problems():
+    """The batching configuration: 512 problems, sizes in {32, ..., 192}^3,
+    codes uniform in 0..4, lambda log-uniform in [-100, -0.01]."""
+    probs = gen.config4_problems(count=512, seed=4)
+    plan = api.BatchPlan(probs)
+    devs = [_dev(p) for p in probs]
+    plan.solve([d[0] for d in devs], [d[1] for d in devs])
+    torch.cuda.synchronize()
+    for i in range(0, 512, 37):
+        assert _rel(devs[i][0].cpu().numpy(), _single(probs[i])) < 1e-13, i
+    plan.close()
+
+
+def test_batch_rejects_bad_plans():
+    with pytest.raises(api.CHZError):
+        api.BatchPlan([dict(nx=8, ny=8, nz=8, xbc=5, ybc=1, zbc=1, lam=-1.0)])
+    with pytest.raises(api.CHZError):
+        api.BatchPlan([dict(nx=7, ny=8, nz=8, xbc=1, ybc=1, zbc=1, lam=-1.0)])
