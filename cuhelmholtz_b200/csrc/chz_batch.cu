@@ -310,12 +310,12 @@ int chz_batch_plan_create(int count, const int* dims, const int* bcs, const doub
     p->ws_bytes = (size_t)ws_total * sizeof(double);
     if (e == cudaSuccess) e = cudaMalloc(&p->ws, p->ws_bytes);
     if (e == cudaSuccess) {
-        for (int q = 0; q < kPasses && e == cudaSuccess; ++q) {
-            e = p->contig[q] ? cudaFuncSetAttribute(batch_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                    (int)p->smem[q])
-                             : cudaFuncSetAttribute(batch_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                    (int)p->smem[q]);
-        }
+        // one attribute per kernel instantiation: the largest need of its passes
+        size_t sc = 0, ss = 0;
+        for (int q = 0; q < kPasses; ++q) (p->contig[q] ? sc : ss) = std::max(p->contig[q] ? sc : ss, p->smem[q]);
+        e = cudaFuncSetAttribute(batch_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(batch_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss);
     }
     if (e != cudaSuccess) {
         const int st = (e == cudaErrorMemoryAllocation) ? fail(CHZ_ERROR_ALLOC, "batch plan allocation failed")
