@@ -482,16 +482,23 @@ fast_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tg, int ntx, int ntil
             // boundary terms: every entry of a y/z boundary row; elsewhere the
             // entries at xs and xe (one thread applies all terms of an entry)
             const BcArgs& b = a.bc;
+            const bool zrow = (v == b.zs || v == b.ze);
+            // rows on a y or z boundary: every entry
             for (int cc = 0; cc < nl; ++cc) {
                 const int j = ub + cc;
-                const bool rowb = (j == b.ys || j == b.ye || v == b.zs || v == b.ze);
-                if (rowb) {
+                if (zrow || j == b.ys || j == b.ye) {
                     for (int l = a.ld_lo + t; l <= a.ld_hi; l += kNT)
                         buf[l * PR + cc] = (T)bc_terms((double)buf[l * PR + cc], b, l, j, v);
-                } else if (t == 2 * cc || (t == 2 * cc + 1 && b.xe != b.xs)) {
-                    const int l = (t & 1) ? b.xe : b.xs;
-                    buf[l * PR + cc] = (T)bc_terms((double)buf[l * PR + cc], b, l, j, v);
                 }
+            }
+            // other rows: the entries at xs and xe, one (row, side) per thread
+            for (int q = t; q < 2 * nl; q += kNT) {
+                const int cc = q >> 1;
+                const int j = ub + cc;
+                if (zrow || j == b.ys || j == b.ye) continue;
+                if ((q & 1) && b.xe == b.xs) continue;
+                const int l = (q & 1) ? b.xe : b.xs;
+                buf[l * PR + cc] = (T)bc_terms((double)buf[l * PR + cc], b, l, j, v);
             }
             __syncthreads();
         }

@@ -81,6 +81,8 @@ def test_matches_oracle_noncubic_mixed_radix(bcs):
 
 
 @pytest.mark.parametrize("dims,bcs,lam", [
+    ((32, 96, 48), (3, 1, 2), -5.0),   # x lines of the 32-point register kernel (128 rows per tile)
+    ((32, 32, 32), (4, 2, 1), -0.5),
     ((64, 64, 64), (1, 2, 0), -2.0),
     ((96, 80, 112), (3, 4, 0), -1.0),
     ((176, 48, 32), (0, 3, 2), -0.01),
