@@ -43,6 +43,11 @@ SIGNATURES = {
                                             c_double, _dp, c_int, c_double,
                                             ctypes.POINTER(c_int), ctypes.POINTER(c_double),
                                             c_void_p, c_size_t, c_void_p]),
+    "chz_helmholtz_adjoint_workspace_size": (c_size_t, [c_int, c_int, c_int, c_int]),
+    "chz_helmholtz_adjoint": (c_int, [c_double, c_double, c_int, c_int, c_double, c_double, c_int, c_int,
+                                      c_double, c_double, c_int, c_int, c_double,
+                                      _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
+                                      c_int, c_int, c_void_p, c_size_t, c_void_p]),
     "chz_batch_plan_create": (c_int, [c_int, ctypes.POINTER(c_int), ctypes.POINTER(c_int),
                                       ctypes.POINTER(c_double), ctypes.POINTER(c_double),
                                       ctypes.POINTER(c_void_p)]),

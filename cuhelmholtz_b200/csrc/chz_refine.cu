@@ -7,6 +7,13 @@
 //
 //   u0 = S32(b);  repeat: r = b - A u (FP64), c = S32(r), u += c
 //
+// Singular case (lambda = 0, every code 0 or 3): the solve removes the
+// constant mode, whose coefficient is the weighted sum 1^T W x over the window
+// (W = 1/2 at Neumann boundary nodes, per axis; 1^T W A = 0).  The residual
+// keeps b's incompatible part c_b = 1^T W b / 1^T W 1 forever, so it is
+// subtracted in FP64 before r is rounded to FP32, and the constant mode that
+// FP32 round-off leaves in u (invisible to the residual) is removed at the end.
+//
 // S32 is the five-pass diagonal solve with FP32 transforms (FP64 tables
 // rounded to FP32, eigenvalue division in FP64); r is formed in FP64 and stored
 // as FP32 straight into the work array, which the next correction's first pass
@@ -29,7 +36,57 @@ struct ResidualArgs {
     float* r;                  // padded (NZ+2)(NY+2)(NX+2)
     double lambda;
     double* sums;              // [0] += r^2, [1] += b^2
+    const double* shift;       // singular case: *shift * inv_w is subtracted from r
+    double inv_w;
 };
+
+// Weight of node (i, j, k) in the constant mode's coefficient.
+__device__ __forceinline__ double mode_weight(const BcArgs& b, int i, int j, int k) {
+    double w = 1.0;
+    if (b.xbc == 3 && (i == 0 || i == b.nx)) w *= 0.5;
+    if (b.ybc == 3 && (j == 0 || j == b.ny)) w *= 0.5;
+    if (b.zbc == 3 && (k == 0 || k == b.nz)) w *= 0.5;
+    return w;
+}
+
+__device__ __forceinline__ void block_add(double v, double* out) {
+    __shared__ double part[32];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) part[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        v = lane < (int)(blockDim.x >> 5) ? part[lane] : 0.0;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) atomicAdd(out, v);
+    }
+}
+
+// out += 1^T W x over the window, x = b (f with boundary terms) when u is
+// NULL, else u.
+__global__ void mode_sum(BcArgs b, const double* u, double* out) {
+    const int i = b.xs + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = b.ys + blockIdx.y;
+    const int k = b.zs + blockIdx.z;
+    double v = 0.0;
+    if (i <= b.xe) {
+        const long long o = (long long)k * (b.nx + 1) * (b.ny + 1) + (long long)j * (b.nx + 1) + i;
+        v = mode_weight(b, i, j, k) * (u ? u[o] : bc_terms(b.f[o], b, i, j, k));
+    }
+    block_add(v, out);
+}
+
+// u -= (*sum) * inv_w on the window.
+__global__ void remove_mode(double* u, BcArgs b, const double* sum, double inv_w) {
+    const int i = b.xs + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = b.ys + blockIdx.y;
+    const int k = b.zs + blockIdx.z;
+    if (i > b.xe) return;
+    const long long o = (long long)k * (b.nx + 1) * (b.ny + 1) + (long long)j * (b.nx + 1) + i;
+    u[o] -= *sum * inv_w;
+}
 
 // r = b - A u at the unknown nodes, with A's homogeneous closures: Dirichlet
 // neighbours are 0 (their values are in b), a Neumann ghost mirrors the
@@ -82,7 +139,7 @@ __global__ void residual_kernel(ResidualArgs a) {
         const double au = (((ul - 2.0 * uc + ur) * b.dx2 + (dl - 2.0 * uc + dr) * b.dy2) +
                            (fl - 2.0 * uc + fr) * b.dz2) + a.lambda * uc;
         const double bv = bc_terms(__ldg(b.f + o), b, i, j, k);
-        const double rv = bv - au;
+        const double rv = a.shift ? (bv - au) - *a.shift * a.inv_w : bv - au;
         const long long wy = b.nx + 2, wz = (long long)(b.nx + 2) * (b.ny + 2);
         a.r[k * wz + j * wy + i] = (float)rv;
         r2 = rv * rv;
@@ -270,7 +327,7 @@ extern "C" int chz_helmholtz_solve_refined(double left, double right, int nx, in
     const size_t wbytes = round256(padded_elems(nx, ny, nz) * sizeof(float));
     double* u = reinterpret_cast<double*>(base + wbytes);
     const size_t ubytes = round256((size_t)(nx + 1) * (ny + 1) * (nz + 1) * sizeof(double));
-    double* sums = reinterpret_cast<double*>(base + wbytes + ubytes);
+    double* sums = reinterpret_cast<double*>(base + wbytes + ubytes);  // [0..1] norms, [2] b's mode, [3] u's
 
     DeviceLineTables tx, ty, tz;
     if ((rc = tables_for(nx, 0, &tx)) || (rc = tables_for(ny, 0, &ty)) || (rc = tables_for(nz, 0, &tz))) return rc;
@@ -287,6 +344,9 @@ extern "C" int chz_helmholtz_solve_refined(double left, double right, int nx, in
     bc.bcl = bcl; bc.bcr = bcr; bc.bcb = bcb; bc.bct = bct; bc.bcf = bcf; bc.bce = bce;
 
     const bool track = tol > 0.0 || rel_residual != nullptr;
+    const bool singular = lambda == 0.0 && (X.bc == 0 || X.bc == 3) && (Y.bc == 0 || Y.bc == 3) &&
+                          (Z.bc == 0 || Z.bc == 3);
+    const double inv_w = 1.0 / ((double)nx * (double)ny * (double)nz);  // 1^T W 1 over the window
     int done = 0;
     double last_rel = -1.0;
     // initial FP32 solve: into f directly when there is nothing to refine
@@ -296,6 +356,12 @@ extern "C" int chz_helmholtz_solve_refined(double left, double right, int nx, in
         if ((rc = solve32_passes(X, Y, Z, tx, ty, tz, ex, ey, ez, lambda, &bc, f, w, u, nullptr, s))) return rc;
         const dim3 rblock(128, 1, 1);
         const dim3 rgrid((X.e - X.s + 1 + 127) / 128, Y.e - Y.s + 1, Z.e - Z.s + 1);
+        if (singular) {
+            cudaError_t e = cudaMemsetAsync(sums + 2, 0, 2 * sizeof(double), s);
+            if (e != cudaSuccess) return cuda_fail((int)e, "memset");
+            mode_sum<<<rgrid, rblock, 0, s>>>(bc, nullptr, sums + 2);
+            count_launch();
+        }
         double prev = -1.0;
         bool copied = false;
         for (int it = 0; it < max_corrections; ++it) {
@@ -305,6 +371,8 @@ extern "C" int chz_helmholtz_solve_refined(double left, double right, int nx, in
             ra.r = w;
             ra.lambda = lambda;
             ra.sums = track ? sums : nullptr;
+            ra.shift = singular ? sums + 2 : nullptr;
+            ra.inv_w = inv_w;
             if (track) {
                 cudaError_t e = cudaMemsetAsync(sums, 0, 2 * sizeof(double), s);
                 if (e != cudaSuccess) return cuda_fail((int)e, "memset");
@@ -338,6 +406,14 @@ extern "C" int chz_helmholtz_solve_refined(double left, double right, int nx, in
             ++done;
         }
         (void)copied;
+        if (singular) {
+            mode_sum<<<rgrid, rblock, 0, s>>>(bc, f, sums + 3);
+            remove_mode<<<rgrid, rblock, 0, s>>>(f, bc, sums + 3, inv_w);
+            count_launch();
+            count_launch();
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) return cuda_fail((int)e, "constant mode");
+        }
     }
     rc = launch_periodic_fixup(f, nx, ny, nz, X.bc, Y.bc, Z.bc, s);
     if (rc) return cuda_fail(rc, "periodic planes");

@@ -93,6 +93,27 @@ int chz_helmholtz_solve_ws(double left, double right, int nx, int xbc,
                            double lambda, double* f,
                            void* workspace, size_t workspace_bytes, void* stream);
 
+/* Adjoint of the solve map (no counterpart in the reference).  The forward
+ * map is the whole in-place API map of chz_helmholtz_solve: f (with its
+ * Dirichlet faces), the six Neumann arrays and lambda -> u.  Given
+ * g = dL/du (full (NZ+1)(NY+1)(NX+1) grid) and the forward solution u, writes
+ * dL/df into df (full grid), dL/d(Neumann array) into dbcl..dbce (each may be
+ * NULL; entries the solve does not read get 0) and, if dlambda is not NULL,
+ * dL/dlambda into the device scalar *dlambda.  A^-T = W A^-1 W^-1 with W =
+ * 1/2 at Neumann boundary nodes, so the work is one homogeneous solve
+ * (precision 0: FP64; 1: FP32 + `corrections` FP64 refinements) between two
+ * scalings.  workspace: at least chz_helmholtz_adjoint_workspace_size bytes,
+ * 256-byte aligned.  All pointers are device pointers. */
+size_t chz_helmholtz_adjoint_workspace_size(int nx, int ny, int nz, int precision);
+int chz_helmholtz_adjoint(double left, double right, int nx, int xbc,
+                          double bottom, double top, int ny, int ybc,
+                          double front, double back, int nz, int zbc, double lambda,
+                          const double* g, const double* u, double* df,
+                          double* dbcl, double* dbcr, double* dbcb, double* dbct,
+                          double* dbcf, double* dbce, double* dlambda,
+                          int precision, int corrections,
+                          void* workspace, size_t workspace_bytes, void* stream);
+
 /* Batched FP64 solves: `count` independent problems of any supported sizes,
  * boundary codes, domains and lambdas (no counterpart in the reference, which
  * solves one problem per call).  The plan precomputes every problem's pass

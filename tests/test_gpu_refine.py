@@ -67,6 +67,19 @@ def test_refinement_reaches_fp64(dims, bcs, lam):
     assert errs[2] < TOL, errs
 
 
+@pytest.mark.parametrize("dims,bcs", [((24, 40, 16), (0, 3, 3)), ((32, 32, 32), (0, 0, 0)),
+                                       ((48, 32, 40), (3, 3, 3))])
+def test_refinement_singular(dims, bcs):
+    """lambda = 0 with every code 0 or 3: the constant mode is removed as in the
+    FP64 solve, and the incompatible part of b does not stall the refinement."""
+    p = gen.random_problem(*dims, *bcs, 0.0, seed=sum(dims))
+    p["f"] = p["f"] + 0.7   # a large incompatible (constant) part
+    ref = fp64(p)
+    u, done, _ = refined(p, 3)
+    assert done == 3
+    assert rel(u, ref) < TOL, rel(u, ref)
+
+
 def test_tolerance_mode_stops_and_reports():
     p = gen.random_problem(64, 64, 64, 3, 4, 0, -1.0, seed=3)
     ref = fp64(p)
