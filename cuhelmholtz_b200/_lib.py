@@ -63,6 +63,7 @@ SIGNATURES = {
     "chz_trace_collect": (c_int, [c_char_p, c_size_t]),
     "chz_launch_count": (ctypes.c_ulonglong, []),
     "chz_set_kernel_family": (c_int, [c_int]),
+    "chz_debug_flags": (c_int, [c_int]),
 }
 
 

@@ -200,10 +200,27 @@ class BatchPlan:
             pass
 
 
-def set_kernel_family(generic_only: bool) -> bool:
-    """Selects the register-resident kernels (default) or the generic
-    mixed-radix kernel for every length; returns the previous setting."""
-    return bool(_lib.lib().chz_set_kernel_family(1 if generic_only else 0))
+KERNEL_FAMILIES = {"default": 0, "generic": 1, "no_tma": 2}
+
+
+def set_kernel_family(family) -> int:
+    """Selects the kernels: "default" (0: TMA-pipelined strided passes,
+    register-resident line kernels, mixed-radix elsewhere), "generic" (1, or
+    True: the mixed-radix kernel for every pass) or "no_tma" (2).  Returns the
+    previous setting (an int, accepted back)."""
+    if isinstance(family, str):
+        family = KERNEL_FAMILIES[family]
+    elif isinstance(family, bool):
+        family = 1 if family else 0
+    prev = _lib.lib().chz_set_kernel_family(int(family))
+    if prev < 0:
+        raise ValueError(f"unknown kernel family {family!r}")
+    return prev
+
+
+def debug_flags(reset: bool = True) -> int:
+    """Flags raised by the kernels' bounded waits (0: none ran out)."""
+    return int(_lib.lib().chz_debug_flags(1 if reset else 0))
 
 
 def workspace_size(NX: int, NY: int, NZ: int, precision: int = 0) -> int:

@@ -477,7 +477,9 @@ size_t chz_helmholtz_workspace_size(int nx, int ny, int nz, int precision) {
         // FP32 work array + FP64 solution array + two FP64 norm accumulators,
         // each piece 256-byte aligned
         auto r256 = [](size_t b) { return (b + 255) & ~(size_t)255; };
-        bytes = r256(pe * sizeof(float)) + r256((size_t)(nx + 1) * (ny + 1) * (nz + 1) * sizeof(double)) + 256;
+        // (FP32 rows padded to a multiple of 4 values: 16-byte row pitch)
+        const size_t pe32 = (size_t)((nx + 2 + 3) & ~3) * (ny + 2) * (nz + 2);
+        bytes = r256(pe32 * sizeof(float)) + r256((size_t)(nx + 1) * (ny + 1) * (nz + 1) * sizeof(double)) + 256;
     }
     return (bytes + 255) & ~(size_t)255;
 }

@@ -28,19 +28,35 @@ namespace fast {
 constexpr int kNT = 128;  // threads per CTA
 constexpr int kR = 16;    // complex values per thread
 
-template <int M>
-struct Cfg {
+// Geometry of a tile of W lines transformed by P = M/16 threads each: the real
+// view of entry l of line c is buf[l * PR + c], the complex view of entry m is
+// Z[m * W + c].  BAR = 0 synchronises the CTA with __syncthreads; BAR > 0 uses
+// named barrier BAR over the NT compute threads only.
+template <int M_, int W_, int PR_, int BAR_>
+struct LineCfg {
+    static constexpr int M = M_;
     static constexpr int P = M / kR;      // threads per line
-    static constexpr int W = kNT / P;     // lines per tile
+    static constexpr int W = W_;          // lines per tile
+    static constexpr int NT = P * W;      // compute threads
     static constexpr int N = 2 * M;
     static constexpr int L = N + 2;       // padded line
-    static constexpr int PR = W + 1;      // real-view pitch (odd: conflict-free transposed access)
+    static constexpr int PR = PR_;        // real-view pitch
+    static constexpr int BAR = BAR_;
     static constexpr int A16 = (M >= 256) ? 2 : 1;               // radix-16 stages
     static constexpr int R0 = M / (A16 == 2 ? 256 : 16);          // last radix (1 = none)
     static constexpr int NST = A16 + (R0 > 1 ? 1 : 0);
     static constexpr int BUF = ((L * PR) + 3) & ~3;   // elements per tile buffer (>= 2*M*W)
     static constexpr int RED = P * W;      // DCT1 odd-sum partials
+    __device__ static __forceinline__ void sync() {
+        if constexpr (BAR == 0) __syncthreads();
+        else asm volatile("bar.sync %0, %1;\n" ::"n"(BAR), "n"(NT) : "memory");
+    }
 };
+
+// The persistent cp.async kernel: 128 threads, odd pitch W + 1 (conflict-free
+// transposed access).
+template <int M>
+using Cfg = LineCfg<M, kNT / (M / kR), kNT / (M / kR) + 1, 0>;
 
 #define CHZ_C1 0.92387953251128675613
 #define CHZ_S1 0.38268343236508977173
@@ -128,10 +144,9 @@ __device__ __forceinline__ void stage_compute(C2<T>* v, int slot, const C2<T>* _
 
 // Complex value A[n] fed to the FFT, from the real view (pre step); the kind
 // is a compile-time constant so the gathers fold to fixed offsets.
-template <typename T, int KIND, int M>
+template <typename T, int KIND, int M, int PR>
 __device__ __forceinline__ C2<T> pre_value(const T* __restrict__ Rv, int c, int n, const LineTables<T>& tb) {
     constexpr int N = 2 * M;
-    constexpr int PR = Cfg<M>::PR;
     if constexpr (KIND == kR2C || KIND == kDCT2 || KIND == kDST2) {
         return mk<T>(fwd_gather<T>(KIND, Rv, PR, c, 2 * n, N, M), fwd_gather<T>(KIND, Rv, PR, c, 2 * n + 1, N, M));
     } else {
@@ -179,10 +194,10 @@ struct OutSink {
 
 // One complete real transform of the W lines held in `buf` (real view in,
 // real view out).
-template <typename T, int M, int KIND, typename SINK>
+template <typename T, typename CF, int KIND, typename SINK>
 __device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot, const LineTables<T>& tb,
                                                 const SINK& sink) {
-    using CF = Cfg<M>;
+    constexpr int M = CF::M;
     constexpr int W = CF::W, PR = CF::PR, N = CF::N, P = CF::P;
     constexpr bool FWD = (KIND == kR2C || KIND == kDCT2 || KIND == kDST2);
     C2<T>* Z = reinterpret_cast<C2<T>*>(buf);
@@ -200,8 +215,8 @@ __device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot,
     {
         using BF = Bfly<M, 0>;
 #pragma unroll
-        for (int k = 0; k < kR; ++k) v[k] = pre_value<T, KIND, M>(buf, c, BF::in_idx(slot, 0, k), tb);
-        __syncthreads();
+        for (int k = 0; k < kR; ++k) v[k] = pre_value<T, KIND, M, PR>(buf, c, BF::in_idx(slot, 0, k), tb);
+        CF::sync();
         stage_compute<T, M, 0>(v, slot, tb.twM);
     }
 
@@ -212,12 +227,12 @@ __device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot,
         _Pragma("unroll") for (int b = 0; b < PB::B; ++b)                                     \
             _Pragma("unroll") for (int k = 0; k < PB::r; ++k)                                 \
                 Z[PB::out_idx(slot, b, k) * W + c] = v[b * PB::r + k];                        \
-        __syncthreads();                                                                      \
+        CF::sync();                                                                      \
         using BF = Bfly<M, S>;                                                                \
         _Pragma("unroll") for (int b = 0; b < BF::B; ++b)                                     \
             _Pragma("unroll") for (int k = 0; k < BF::r; ++k)                                 \
                 v[b * BF::r + k] = Z[BF::in_idx(slot, b, k) * W + c];                         \
-        __syncthreads();                                                                      \
+        CF::sync();                                                                      \
         stage_compute<T, M, S>(v, slot, tb.twM);                                              \
     }
     CHZ_STAGE(1)
@@ -232,7 +247,7 @@ __device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot,
         for (int b = 0; b < LB::B; ++b)
 #pragma unroll
             for (int k = 0; k < LB::r; ++k) Z[LB::out_idx(slot, b, k) * W + c] = v[b * LB::r + k];
-        __syncthreads();
+        CF::sync();
     }
     if constexpr (FWD) {
         // split: V[m] = 1/2 (Z[m] + conj Z[M-m]) - i/2 w^m (Z[m] - conj Z[M-m])
@@ -250,7 +265,7 @@ __device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot,
                 v[b * LB::r + k] = mk<T>(T(0.5) * (e.x + o.y), T(0.5) * (e.y - o.x));
                 if (m == 0) vM = mk<T>(zk.x - zk.y, T(0));
             }
-        __syncthreads();
+        CF::sync();
 #pragma unroll
         for (int b = 0; b < LB::B; ++b)
 #pragma unroll
@@ -322,7 +337,7 @@ __device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot,
                 outs[2 * (b * LB::r + k)] = oe;
                 outs[2 * (b * LB::r + k) + 1] = oo;
             }
-        __syncthreads();
+        CF::sync();
 #pragma unroll
         for (int b = 0; b < LB::B; ++b)
 #pragma unroll
@@ -360,7 +375,7 @@ __device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot,
                 }
             }
     }
-    __syncthreads();
+    CF::sync();
 }
 
 template <int KIND, int N>
@@ -514,16 +529,16 @@ fast_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tg, int ntx, int ntil
             s1.dlo = a.dv.lo;
             s1.dhi = a.dv.hi;
             s1.zmax = (a.dv.perturb && i <= a.dv.xz_hi && v <= a.dv.yz_hi) ? a.dv.zz_hi : -1;
-            transform_lines<T, M, KIND>(buf, red, c, slot, tb, s1);
+            transform_lines<T, CF, KIND>(buf, red, c, slot, tb, s1);
             OutSink<T, PR, false> s2;
             s2.Rv = buf;
             s2.c = c;
-            transform_lines<T, M, KIND2>(buf, red, c, slot, tb, s2);
+            transform_lines<T, CF, KIND2>(buf, red, c, slot, tb, s2);
         } else {
             OutSink<T, PR, false> s;
             s.Rv = buf;
             s.c = c;
-            transform_lines<T, M, KIND>(buf, red, c, slot, tb, s);
+            transform_lines<T, CF, KIND>(buf, red, c, slot, tb, s);
         }
 
         // ---- store the output window ----

@@ -298,10 +298,38 @@ static int launch_fast_t(bool contig, const void* in, void* out, const PassArgs&
 #undef CHZ_M
 }
 
+namespace tma {
+template <typename T, int M>
+int launch_tma_kind(int kind, int kind2, const void* in, void* out, const PassArgs& a, const LineTables<T>& tb,
+                    int nv, cudaStream_t stream, const char* label);
+}  // namespace tma
+
+// Strided passes of N = 128, 256, 512 with the same type in and out and no
+// scale, accumulation or boundary terms go to the TMA-pipelined kernel; -1
+// when it does not take the pass.
+template <typename T>
+static int try_tma(const void* in, void* out, const PassArgs& a, const DeviceLineTables& tb, int nv,
+                   cudaStream_t stream, const char* label) {
+    if (a.acc || a.use_scale || a.has_bc) return -1;
+    const LineTables<T> t = to_tables<T>(tb);
+    switch (tb.M) {
+        case 64: return tma::launch_tma_kind<T, 64>(a.kind, a.kind2, in, out, a, t, nv, stream, label);
+        case 128: return tma::launch_tma_kind<T, 128>(a.kind, a.kind2, in, out, a, t, nv, stream, label);
+        case 256: return tma::launch_tma_kind<T, 256>(a.kind, a.kind2, in, out, a, t, nv, stream, label);
+        default: return -1;
+    }
+}
+
 int launch_line_pass(int is_double, int in_type, int out_type, bool contig, const void* in,
                      void* out, const PassArgs& a, const DeviceLineTables& tb, const LineGeom& g,
                      int nv, cudaStream_t stream, const char* label) {
-    if (fast_path_supported(tb.M) && !g_force_generic) {
+    const int family = g_force_generic.load(std::memory_order_relaxed);
+    if (!contig && family == 0 && in_type == out_type) {
+        const int rc = is_double ? try_tma<double>(in, out, a, tb, nv, stream, label)
+                                 : try_tma<float>(in, out, a, tb, nv, stream, label);
+        if (rc != -1) return rc;
+    }
+    if (fast_path_supported(tb.M) && family != 1) {
         if (is_double) {
             if (in_type == kIoF64 && out_type == kIoF64)
                 return launch_fast_t<double, double, double>(contig, in, out, a, tb, nv, stream, label);
@@ -447,7 +475,10 @@ int chz_trace_collect(char* buf, size_t len) {
 // Selects the kernel family: 0 = register-resident kernels where supported
 // (default), 1 = the generic shared-memory kernel for every length.  Returns
 // the previous setting.
-int chz_set_kernel_family(int generic_only) { return g_force_generic.exchange(generic_only ? 1 : 0); }
+int chz_set_kernel_family(int family) {
+    if (family < 0 || family > 2) return -1;
+    return g_force_generic.exchange(family);
+}
 
 // Total kernel launches issued by this library in this process.
 unsigned long long chz_launch_count(void) { return launch_count(); }

@@ -33,12 +33,17 @@ namespace {
 struct ResidualArgs {
     BcArgs bc;                 // b = f + boundary terms
     const double* u;           // (NZ+1)(NY+1)(NX+1), same layout as f
-    float* r;                  // padded (NZ+2)(NY+2)(NX+2)
+    float* r;                  // padded (NZ+2)(NY+2)(pitch32(NX)) work array
+    long long ry, rz;          // its row and plane pitch
     double lambda;
     double* sums;              // [0] += r^2, [1] += b^2
     const double* shift;       // singular case: *shift * inv_w is subtracted from r
     double inv_w;
 };
+
+// Row pitch (values) of the FP32 work array: NX + 2 rounded up to a multiple
+// of 4, so that rows start on 16-byte boundaries (bulk tensor copies).
+__host__ __device__ __forceinline__ long long pitch32(int nx) { return (nx + 2 + 3) & ~3; }
 
 // Weight of node (i, j, k) in the constant mode's coefficient.
 __device__ __forceinline__ double mode_weight(const BcArgs& b, int i, int j, int k) {
@@ -140,8 +145,7 @@ __global__ void residual_kernel(ResidualArgs a) {
                            (fl - 2.0 * uc + fr) * b.dz2) + a.lambda * uc;
         const double bv = bc_terms(__ldg(b.f + o), b, i, j, k);
         const double rv = a.shift ? (bv - au) - *a.shift * a.inv_w : bv - au;
-        const long long wy = b.nx + 2, wz = (long long)(b.nx + 2) * (b.ny + 2);
-        a.r[k * wz + j * wy + i] = (float)rv;
+        a.r[k * a.rz + j * a.ry + i] = (float)rv;
         r2 = rv * rv;
         b2 = bv * bv;
     }
@@ -196,7 +200,7 @@ int solve32_passes(const AxisSolve& X, const AxisSolve& Y, const AxisSolve& Z, c
     int rc;
     const int nx = X.n, ny = Y.n, nz = Z.n;
     const long long fy = nx + 1, fz = (long long)(nx + 1) * (ny + 1);
-    const long long wy = nx + 2, wz = (long long)(nx + 2) * (ny + 2);
+    const long long wy = pitch32(nx), wz = wy * (ny + 2);
     {
         const LineGeom g = line_geometry(nx, 0, true);
         PassArgs a{};
@@ -324,7 +328,7 @@ extern "C" int chz_helmholtz_solve_refined(double left, double right, int nx, in
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     char* base = static_cast<char*>(workspace);
     float* w = reinterpret_cast<float*>(base);
-    const size_t wbytes = round256(padded_elems(nx, ny, nz) * sizeof(float));
+    const size_t wbytes = round256((size_t)pitch32(nx) * (ny + 2) * (nz + 2) * sizeof(float));
     double* u = reinterpret_cast<double*>(base + wbytes);
     const size_t ubytes = round256((size_t)(nx + 1) * (ny + 1) * (nz + 1) * sizeof(double));
     double* sums = reinterpret_cast<double*>(base + wbytes + ubytes);  // [0..1] norms, [2] b's mode, [3] u's
@@ -369,6 +373,8 @@ extern "C" int chz_helmholtz_solve_refined(double left, double right, int nx, in
             ra.bc = bc;
             ra.u = u;
             ra.r = w;
+            ra.ry = pitch32(nx);
+            ra.rz = pitch32(nx) * (ny + 2);
             ra.lambda = lambda;
             ra.sums = track ? sums : nullptr;
             ra.shift = singular ? sums + 2 : nullptr;

@@ -1,0 +1,269 @@
+// TMA-pipelined line pass for the strided axes (y and z passes).
+//
+// A tile is W adjacent x columns (128 bytes: 16 FP64 or 32 FP32 values) of
+// the lines of one plane; a line runs along y or z.  One producer thread
+// moves whole tiles with cp.async.bulk.tensor: loads land in one of S stage
+// buffers (row l of the tile at shared row l, so the kind's input window is
+// addressed directly; rows the pass does not load are filled with zeros by
+// the copy engine, which also zero-fills columns past the last line), and
+// finished tiles leave by bulk tensor stores clipped to the output window.
+// The compute warps run the register-resident radix-16 line transform of
+// chz_fast.cuh on the stage buffer in place, synchronised by a named barrier
+// that leaves the producer warp out, so loads run up to S - 1 tiles ahead of
+// the compute and stores drain behind it.
+//
+// Every entry of a 128-byte row is read or written by the W threads of one
+// slot at once, so all shared accesses of the real view are bank-conflict
+// free; the complex exchange view Z[m * W + c] is two rows per entry.
+//
+// Waits are bounded: a wait that runs out sets a flag that the host can read
+// (chz_debug_flags) and the thread carries on, so the kernel always ends.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "chz_fast.cuh"
+
+namespace chz {
+namespace tma {
+
+using fast::LineCfg;
+using fast::OutSink;
+using fast::transform_lines;
+
+template <typename T>
+struct TileW {
+    static constexpr int W = 128 / (int)sizeof(T);
+};
+
+template <typename T, int M>
+using TCfg = LineCfg<M, TileW<T>::W, TileW<T>::W, 1>;
+
+constexpr int kStages = 3;
+
+// Host-computed geometry of one pass.
+struct TmaGeom {
+    int rows_buf;     // rows of one stage buffer
+    int ld_row0;      // shared row of the first loaded row
+    int ld_coord0;    // its line coordinate in the load map
+    int ld_nch;       // boxes per tile load
+    int ld_box;       // rows per load box
+    int st_row0;      // shared row of the first stored row
+    int st_nch;       // boxes per tile store
+    int st_box;       // rows per store box
+    int l_mid;        // 1: map dims (u, l, v); 0: (u, v, l)
+    unsigned tx_bytes;  // bytes one tile load delivers
+    int col0;         // u of map column 0
+};
+
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(saddr(b)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(saddr(b)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(saddr(b)) : "memory");
+}
+
+// Waits for the phase with the given parity to complete.  Gives up after
+// about a second of SM clock, or at once when another thread of the CTA has
+// given up (*abort), so a CTA whose copies never arrive still ends quickly.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort) {
+    const uint32_t a = saddr(b);
+    const long long t0 = clock64();
+    while (true) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (*abort || clock64() - t0 > 2000000000LL) {
+            *abort = 1;
+            return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load(void* dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(
+            saddr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(saddr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_store(const CUtensorMap* map, int c0, int c1, int c2, const void* src) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];\n" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(c0), "r"(c1), "r"(c2), "r"(saddr(src))
+                 : "memory");
+}
+
+// Shared-memory carve-up (byte offsets).
+template <typename T, int M, bool FUSED>
+struct TmaSmem {
+    using CF = TCfg<T, M>;
+    __host__ __device__ static constexpr size_t al(size_t b, size_t a) { return (b + a - 1) / a * a; }
+    __host__ __device__ static size_t stage_bytes(int rows_buf) { return (size_t)rows_buf * CF::W * sizeof(T); }
+    __host__ __device__ static size_t twM(int rows_buf) { return al(kStages * stage_bytes(rows_buf), 128); }
+    __host__ __device__ static size_t twN(int rows_buf) { return twM(rows_buf) + sizeof(C2<T>) * M; }
+    __host__ __device__ static size_t tw4N(int rows_buf) { return twN(rows_buf) + sizeof(C2<T>) * (M + 1); }
+    __host__ __device__ static size_t inv4sin(int rows_buf) { return tw4N(rows_buf) + sizeof(C2<T>) * (M + 1); }
+    __host__ __device__ static size_t ez(int rows_buf) { return al(inv4sin(rows_buf) + sizeof(T) * (M + 1), 16); }
+    __host__ __device__ static size_t red(int rows_buf) {
+        return al(ez(rows_buf) + (FUSED ? sizeof(double) * (2 * M + 2) : 0), 16);
+    }
+    __host__ __device__ static size_t bars(int rows_buf) { return al(red(rows_buf) + sizeof(T) * CF::RED, 16); }
+    __host__ __device__ static size_t abort(int rows_buf) { return bars(rows_buf) + 2 * kStages * sizeof(uint64_t); }
+    __host__ __device__ static size_t total(int rows_buf) { return abort(rows_buf) + 16; }
+};
+
+template <typename T, int M, int KIND, int KIND2>
+__global__ void __launch_bounds__(TCfg<T, M>::NT + 32, 1)
+tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUtensorMap stmap, PassArgs a,
+         LineTables<T> tg, TmaGeom g, int ntx, int ntiles, int* flags) {
+    using CF = TCfg<T, M>;
+    using SL = TmaSmem<T, M, (KIND2 >= 0)>;
+    constexpr int W = CF::W, PR = CF::PR, NT = CF::NT, N = CF::N;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int t = threadIdx.x;
+    if ((int)blockIdx.x >= ntiles) return;
+    if (saddr(smem_raw) & 127) {  // uniform over the CTA: nothing has started
+        if (t == 0) atomicOr(flags, 4);
+        return;
+    }
+    const int rb = g.rows_buf;
+    const size_t sbytes = SL::stage_bytes(rb);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + SL::bars(rb));
+    uint64_t* ready = full + kStages;
+    volatile int* abort = reinterpret_cast<volatile int*>(smem_raw + SL::abort(rb));
+    T* red = reinterpret_cast<T*>(smem_raw + SL::red(rb));
+
+    LineTables<T> tb = tg;
+    {
+        C2<T>* sM = reinterpret_cast<C2<T>*>(smem_raw + SL::twM(rb));
+        C2<T>* sN = reinterpret_cast<C2<T>*>(smem_raw + SL::twN(rb));
+        C2<T>* s4 = reinterpret_cast<C2<T>*>(smem_raw + SL::tw4N(rb));
+        T* sI = reinterpret_cast<T*>(smem_raw + SL::inv4sin(rb));
+        for (int i = t; i < M; i += blockDim.x) sM[i] = tg.twM[i];
+        for (int i = t; i <= M; i += blockDim.x) {
+            sN[i] = tg.twN[i];
+            s4[i] = tg.tw4N[i];
+            sI[i] = tg.inv4sin[i];
+        }
+        tb.twM = sM;
+        tb.twN = sN;
+        tb.tw4N = s4;
+        tb.inv4sin = sI;
+    }
+    double* ez_s = reinterpret_cast<double*>(smem_raw + SL::ez(rb));
+    if constexpr (KIND2 >= 0) {
+        for (int i = t; i < N + 2; i += blockDim.x) ez_s[i] = a.dv.ez[i];
+    }
+    if (t == 0) {
+        *abort = 0;
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(full + s, 1);
+            mbar_init(ready + s, NT);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+
+    const int nloc = (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1;
+
+    if (t >= NT) {
+        // ---------------- producer ----------------
+        if (t != NT) return;
+        asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&ldmap)) : "memory");
+        asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&stmap)) : "memory");
+        auto issue_load = [&](int i) {
+            const int s = i % kStages;
+            const int tile = (int)blockIdx.x + i * (int)gridDim.x;
+            const int cx = (tile % ntx) * W;
+            const int v = a.v0 + tile / ntx;
+            unsigned char* dst = smem_raw + (size_t)s * sbytes;
+            mbar_expect_tx(full + s, g.tx_bytes);
+            for (int q = 0; q < g.ld_nch; ++q) {
+                const int l = g.ld_coord0 + q * g.ld_box;
+                void* d = dst + (size_t)(g.ld_row0 + q * g.ld_box) * W * sizeof(T);
+                if (g.l_mid) tma_load(d, &ldmap, cx, l, v, full + s);
+                else tma_load(d, &ldmap, cx, v, l, full + s);
+            }
+        };
+        const int pre = nloc < kStages ? nloc : kStages;
+        for (int i = 0; i < pre; ++i) issue_load(i);
+        for (int i = 0; i < nloc; ++i) {
+            const int s = i % kStages;
+            if (!mbar_wait(ready + s, (uint32_t)((i / kStages) & 1), abort)) atomicOr(flags, 1);
+            const int tile = (int)blockIdx.x + i * (int)gridDim.x;
+            const int cx = (tile % ntx) * W;
+            const int v = a.v0 + tile / ntx;
+            const unsigned char* src = smem_raw + (size_t)s * sbytes;
+            for (int q = 0; q < g.st_nch; ++q) {
+                const int l = q * g.st_box;
+                const void* sp = src + (size_t)(g.st_row0 + q * g.st_box) * W * sizeof(T);
+                if (g.l_mid) tma_store(&stmap, cx, l, v, sp);
+                else tma_store(&stmap, cx, v, l, sp);
+            }
+            asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+            if (i + kStages < nloc) {
+                // the buffer is refilled once the store has read it
+                asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+                issue_load(i + kStages);
+            }
+        }
+        asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+        return;
+    }
+
+    // ---------------- compute ----------------
+    const int c = t % W;
+    const int slot = t / W;
+    for (int i = 0; i < nloc; ++i) {
+        const int s = i % kStages;
+        if (!mbar_wait(full + s, (uint32_t)((i / kStages) & 1), abort)) {
+            if (t == 0) atomicOr(flags, 2);
+        }
+        T* buf = reinterpret_cast<T*>(smem_raw + (size_t)s * sbytes);
+        const int tile = (int)blockIdx.x + i * (int)gridDim.x;
+        const int v = a.v0 + tile / ntx;
+        if constexpr (KIND2 >= 0) {
+            OutSink<T, PR, true> s1;
+            s1.Rv = buf;
+            s1.c = c;
+            int col = g.col0 + (tile % ntx) * W + c;
+            col = max(a.u0, min(col, a.u0 + a.nu - 1));
+            s1.exy = __ldg(a.dv.ex + col) + __ldg(a.dv.ey + v);
+            s1.lam = a.dv.lambda;
+            s1.ez = ez_s;
+            s1.dlo = a.dv.lo;
+            s1.dhi = a.dv.hi;
+            s1.zmax = (a.dv.perturb && col <= a.dv.xz_hi && v <= a.dv.yz_hi) ? a.dv.zz_hi : -1;
+            transform_lines<T, CF, KIND>(buf, red, c, slot, tb, s1);
+            OutSink<T, PR, false> s2;
+            s2.Rv = buf;
+            s2.c = c;
+            transform_lines<T, CF, KIND2>(buf, red, c, slot, tb, s2);
+        } else {
+            OutSink<T, PR, false> sk;
+            sk.Rv = buf;
+            sk.c = c;
+            transform_lines<T, CF, KIND>(buf, red, c, slot, tb, sk);
+        }
+        // make this thread's writes visible to the bulk store, then release
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_arrive(ready + s);
+    }
+}
+
+}  // namespace tma
+}  // namespace chz

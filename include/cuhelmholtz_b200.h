@@ -194,11 +194,18 @@ int chz_release_cached(void);
 int chz_trace_enable(int on);
 int chz_trace_collect(char* buf, size_t len);
 
-/* Kernel family: 0 (default) uses the register-resident line kernels for
- * lengths N = 32..1024 that are powers of two and the shared-memory mixed-radix
- * kernel elsewhere; 1 uses the mixed-radix kernel for every length (both are
- * checked against the same oracle).  Returns the previous setting. */
-int chz_set_kernel_family(int generic_only);
+/* Kernel family: 0 (default) uses the TMA-pipelined kernel for the strided
+ * (y, z) passes of N = 128, 256, 512, the register-resident line kernels for
+ * the other passes of lengths N = 32..1024 that are powers of two, and the
+ * shared-memory mixed-radix kernel elsewhere; 1 uses the mixed-radix kernel
+ * for every pass; 2 is family 0 without the TMA kernel (all are checked
+ * against the same oracle).  Returns the previous setting, or -1 for an
+ * unknown family. */
+int chz_set_kernel_family(int family);
+
+/* Flags raised by the kernels' bounded waits since the last reset (0 when no
+ * wait ran out); reset != 0 clears them.  Synchronous.  -1 on a CUDA error. */
+int chz_debug_flags(int reset);
 
 /* Number of kernel launches this library has issued in this process. */
 unsigned long long chz_launch_count(void);

@@ -117,12 +117,14 @@ def test_config3_512_manufactured_exact():
     assert err < TOL, err
 
 
+@pytest.mark.parametrize("family", ["generic", "no_tma"])
 @pytest.mark.parametrize("bcs", [(1, 2, 0), (3, 4, 0), (0, 0, 0), (2, 1, 4), (4, 3, 2), (1, 1, 1), (3, 3, 3)])
-def test_kernel_families_agree(bcs):
-    """Register-resident and generic kernels give the same solve (1e-13)."""
+def test_kernel_families_agree(bcs, family):
+    """The TMA-pipelined, register-resident and generic kernels give the same
+    solve (1e-13)."""
     p = gen.random_problem(64, 32, 128, *bcs, -2.0, seed=5)
     a = gpu_solve(p)
-    prev = api.set_kernel_family(True)
+    prev = api.set_kernel_family(family)
     try:
         b = gpu_solve(p)
     finally:
