@@ -38,6 +38,17 @@ WORKLOADS = {
                                    "FP64 Helmholtz solve 256x192x320, BC (2,4,3), f~U[-1,1]"),
 }
 DEFAULT_WORKLOAD = "helmholtz_fp64_512"
+
+# DRAM bytes (read + write) per launch of each pass, from one ncu capture of
+# `bench.py --batch 1 --steps 1 --warmup 3 --e2e-steps 1 --no-cpu-baseline
+# --refine-corrections -1` (profiles/solve_512_passes_ncu.md).
+NCU_TRAFFIC = {
+    ("helmholtz_fp64_512", "solve_x_fwd"): 2126747000,
+    ("helmholtz_fp64_512", "solve_y_fwd"): 2101835000,
+    ("helmholtz_fp64_512", "solve_z_fwd_div_inv"): 2105996000,
+    ("helmholtz_fp64_512", "solve_y_inv"): 2102001000,
+    ("helmholtz_fp64_512", "solve_x_inv"): 2110305000,
+}
 METRIC = "solves/s (FP64 Helmholtz solve)"
 
 
@@ -65,20 +76,20 @@ def _windows(bc, n):
 
 def solve_pass_bytes(nx, ny, nz, xbc, ybc, zbc, esize=8):
     """Bytes each line pass of one solve must read and write (algorithmic:
-    every loaded and stored entry once), in launch order."""
+    every loaded and stored entry once), by trace label, in launch order."""
     xs, xe, xp0, xp1 = _windows(xbc, nx)
     ys, ye, yp0, yp1 = _windows(ybc, ny)
     zs, ze, zp0, zp1 = _windows(zbc, nz)
     X, Xs = xe - xs + 1, xp1 - xp0 + 1
     Y, Ys = ye - ys + 1, yp1 - yp0 + 1
     Z, Zs = ze - zs + 1, zp1 - zp0 + 1
-    return [
-        (Y * Z) * (X + Xs) * esize,    # x forward: f -> work
-        (Xs * Z) * (Y + Ys) * esize,   # y forward
-        (Xs * Ys) * (Z + Z) * esize,   # z forward + divide + z inverse
-        (Xs * Z) * (Ys + Y) * esize,   # y inverse
-        (Y * Z) * (Xs + X) * esize,    # x inverse: work -> f
-    ]
+    return {
+        "solve_x_fwd": (Y * Z) * (X + Xs) * esize,            # f -> work
+        "solve_y_fwd": (Xs * Z) * (Y + Ys) * esize,
+        "solve_z_fwd_div_inv": (Xs * Ys) * (Z + Z) * esize,   # forward, divide, inverse
+        "solve_y_inv": (Xs * Z) * (Ys + Y) * esize,
+        "solve_x_inv": (Y * Z) * (Xs + X) * esize,            # work -> f
+    }
 
 
 # ---------------------------------------------------------------------------
@@ -323,18 +334,21 @@ def run_ours(args):
     _lib.trace_enable(False)
     tr = _lib.trace_collect()
     pass_bytes = solve_pass_bytes(nx, ny, nz, xbc, ybc, zbc)
-    line_labels = ["solve_x_fwd", "solve_y_fwd", "solve_z_fwd_div_inv", "solve_y_inv", "solve_x_inv"]
-    lp_ms = sum(tr[k][1] for k in line_labels if k in tr)
-    lp_n = sum(tr[k][0] for k in line_labels if k in tr)
+    line_labels = [k for k in pass_bytes if k in tr]
+    lp_ms = sum(tr[k][1] for k in line_labels)
+    lp_n = sum(tr[k][0] for k in line_labels)
     nsolves_traced = tsteps * B
-    lp_bytes = sum(pass_bytes) * nsolves_traced
+    lp_bytes = sum(pass_bytes[k] * tr[k][0] for k in line_labels)
     peak, peak_src = measured_peaks()
     achieved = (lp_bytes / (lp_ms / 1000.0)) / 1e9 if lp_ms > 0 else None
     per_pass = {k: {"launches": tr[k][0], "avg_ms": tr[k][1] / tr[k][0],
-                    "gbs": (pass_bytes[i] / (tr[k][1] / tr[k][0] / 1000.0)) / 1e9}
-                for i, k in enumerate(line_labels) if k in tr}
+                    "gbs": (pass_bytes[k] / (tr[k][1] / tr[k][0] / 1000.0)) / 1e9}
+                for k in line_labels}
     total_trace_ms = sum(v[1] for v in tr.values())
-    solve_bytes = sum(pass_bytes)
+    solve_bytes = lp_bytes / nsolves_traced   # bytes of the schedule executed
+    # dominant kernel: the pass with the largest share of the traced time
+    dom_k = max(line_labels, key=lambda k: tr[k][1]) if line_labels else None
+    dom_gbs = per_pass[dom_k]["gbs"] if dom_k else None
 
     # ---- FP32 transforms + FP64 refinement on the same problems ----
     refine = None
@@ -429,10 +443,13 @@ def run_ours(args):
                          f"{npts * 8 / 1e9:.2f} GB each)"},
         "hbm_gbs_solve": (solve_bytes * args.steps * B / (elapsed_ms / 1000.0)) / 1e9,
         "algorithmic_bytes_per_solve": solve_bytes,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": None,
-                     "kernel": "line_pass<double> (5 launches per solve)",
+        "roofline": {"bound": "hbm", "achieved": dom_gbs, "peak": peak, "unit": "GB/s",
+                     "frac": (dom_gbs / peak) if dom_gbs else None,
+                     "traffic": NCU_TRAFFIC.get((name, dom_k)),
+                     "kernel": dom_k, "algorithmic_bytes_per_launch": pass_bytes.get(dom_k),
                      "peak_source": peak_src, "per_pass": per_pass,
+                     "all_passes_gbs": achieved,
+                     "all_passes_frac": (achieved / peak) if achieved else None,
                      "line_pass_share_of_traced_time": lp_ms / total_trace_ms if total_trace_ms else None,
                      "launches_traced": lp_n},
         "cpu_baseline": cpu,

@@ -169,22 +169,40 @@ struct OutSink {
     const double* ez;
     int dlo, dhi;     // spectral window along the line
     int zmax;         // entries l <= zmax are zeroed (zero mode), else -1
+    // 1 / (lambda_x + lambda_y + lambda_z[l] + lambda), 0 for the zero mode
+    __device__ __forceinline__ double eig(int l) const {
+        const double r = recip((exy + ez[l]) + lam);
+        return l <= zmax ? 0.0 : r;
+    }
     __device__ __forceinline__ void put(int l, T val) const {
         if constexpr (DIV) {
-            if (l >= dlo && l <= dhi) {
-                const double den = (exy + ez[l]) + lam;
-                double eig = recip(den);
-                if (l <= zmax) eig = 0.0;
-                val = (T)((double)val * eig);
-            }
+            if (l >= dlo && l <= dhi) val = (T)((double)val * eig(l));
         }
         Rv[l * PR + c] = val;
     }
-    // 1/d: single-precision seed refined by two Newton-Raphson steps
-    // r <- r + r (1 - d r), which square the relative error each time
-    // (2^-23 -> 2^-46 -> below double rounding).
+    // Entries l, l + 1 of one complex bin of a periodic axis, which share the
+    // eigenvalue (one reciprocal for both).
+    __device__ __forceinline__ void put_pair(int l, T re, T im) const {
+        if constexpr (DIV) {
+            if (l >= dlo && l + 1 <= dhi) {
+                const double e = eig(l);
+                re = (T)((double)re * e);
+                im = (T)((double)im * e);
+            } else {
+                put(l, re);
+                put(l + 1, im);
+                return;
+            }
+        }
+        Rv[l * PR + c] = re;
+        Rv[(l + 1) * PR + c] = im;
+    }
+    // 1/d: the hardware's approximate FP64 reciprocal (about 23 good bits)
+    // refined by two Newton-Raphson steps r <- r + r (1 - d r), each of which
+    // squares the relative error (2^-23 -> 2^-46 -> below double rounding).
     __device__ static __forceinline__ double recip(double d) {
-        double r = (double)__frcp_rn((float)d);
+        double r;
+        asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
         double e = fma(-d, r, 1.0);
         r = fma(r, e, r);
         e = fma(-d, r, 1.0);
@@ -273,12 +291,8 @@ __device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot,
                 const int m = LB::out_idx(slot, b, k);
                 const C2<T> V = v[b * LB::r + k];
                 if constexpr (KIND == kR2C) {
-                    sink.put(2 * m, V.x);
-                    sink.put(2 * m + 1, m == 0 ? T(0) : V.y);
-                    if (m == 0) {
-                        sink.put(N, vM.x);
-                        sink.put(N + 1, T(0));
-                    }
+                    sink.put_pair(2 * m, V.x, m == 0 ? T(0) : V.y);
+                    if (m == 0) sink.put_pair(N, vM.x, T(0));
                 } else {
                     const C2<T> a = cmul<T>(ldtw<T>(tb.tw4N + m), V);
                     if constexpr (KIND == kDCT2) {
