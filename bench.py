@@ -509,6 +509,15 @@ def run_batch(args):
     l0 = _lib.launch_count()
     ms = timed(lambda: plan.solve(fs, faces), args.steps)
     launches = _lib.launch_count() - l0
+    targets, tuned_ms = plan.tiles()
+    # the same batch with the untuned tile size (4096 values per tile)
+    prev = chz.BatchPlan.set_autotune(False)
+    try:
+        plain = chz.BatchPlan(probs)
+    finally:
+        chz.BatchPlan.set_autotune(prev)
+    ms_plain = timed(lambda: plain.solve(fs, faces), args.steps)
+    plain.close()
     ms_loop = timed(loop, args.steps)
     value = args.batch_count * args.steps / (ms / 1000.0)
     loop_value = args.batch_count * args.steps / (ms_loop / 1000.0)
@@ -522,6 +531,8 @@ def run_batch(args):
                    "points_per_step": npts},
         "hbm_gbs_model": 80.0 * npts * args.steps / (ms / 1000.0) / 1e9,
         "loop_of_single_solves": {"value": loop_value, "ms_per_step": ms_loop / args.steps},
+        "autotune": {"tile_values_per_pass": targets, "tuned_ms_per_pass": tuned_ms,
+                     "untuned_value": args.batch_count * args.steps / (ms_plain / 1000.0)},
         "speedup_vs_loop": value / loop_value,
         "gpu_launches": int(launches),
     }

@@ -188,6 +188,21 @@ class BatchPlan:
     def workspace_bytes(self) -> int:
         return int(_lib.lib().chz_batch_workspace_bytes(self._handle))
 
+    def tiles(self):
+        """Tile size (values per tile) the autotuner chose for each of the
+        five passes, and the measured time per launch in ms (0: not tuned)."""
+        import ctypes
+        t = (ctypes.c_int * 5)()
+        ms = (ctypes.c_float * 5)()
+        _check(_lib.lib().chz_batch_plan_tiles(self._handle, t, ms))
+        return list(t), [float(v) for v in ms]
+
+    @staticmethod
+    def set_autotune(on: bool) -> bool:
+        """Turns the plans' autotuner on (default) or off; returns the
+        previous setting."""
+        return bool(_lib.lib().chz_batch_set_autotune(1 if on else 0))
+
     def close(self):
         if self._handle:
             _lib.lib().chz_batch_plan_destroy(self._handle)

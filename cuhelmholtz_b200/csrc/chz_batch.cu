@@ -13,6 +13,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <mutex>
 #include <cstring>
 #include <map>
 #include <new>
@@ -137,6 +139,8 @@ struct chz_batch_plan {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaStream_t graph_stream = nullptr;
+    int target[kPasses] = {};            // tile size (values per tile) of each pass
+    float tuned_ms[kPasses] = {};        // its measured time (0: not tuned)
 };
 
 namespace {
@@ -157,17 +161,133 @@ void free_plan(chz_batch_plan* p) {
     delete p;
 }
 
+// One problem's pass before the tile shape is chosen.
+struct PassTemplate {
+    BatchItem it;     // everything but the tile-dependent fields
+    int n;            // line length
+    int nv;           // planes of lines
+};
+
+constexpr size_t kBatchMaxSmem = 110 * 1024;  // two CTAs per SM
+constexpr int kDefaultTarget = 4096;            // values per tile without tuning
+constexpr int kTargets[] = {1024, 2048, 4096, 8192, 16384};
+std::atomic<int> g_autotune{1};
+
+// Fills the tile-dependent fields of pass q for every problem at tile size
+// `target` (values per tile); returns the launch's tile count and shared memory.
+void materialise(const std::vector<PassTemplate>& tp, bool contig, int target, std::vector<BatchItem>& items,
+                 std::vector<int>& start, int* tiles, size_t* smem) {
+    const int count = (int)tp.size();
+    items.resize(count);
+    start.assign(count + 1, 0);
+    *smem = 0;
+    for (int i = 0; i < count; ++i) {
+        const LineGeom g = line_geometry_target(tp[i].n, 1, contig, target, kBatchMaxSmem);
+        BatchItem& it = items[i];
+        it = tp[i].it;
+        it.a.PR = g.PR;
+        it.a.log2W = g.log2W;
+        it.buf_elems = (int)g.buf_elems;
+        it.ntx = (it.a.nu + g.W - 1) / g.W;
+        start[i + 1] = start[i] + it.ntx * tp[i].nv;
+        *smem = std::max(*smem, g.smem_bytes);
+    }
+    *tiles = start[count];
+}
+
+cudaError_t launch_pass(chz_batch_plan* p, int q, cudaStream_t s) {
+    if (p->tiles[q] == 0) return cudaSuccess;
+    if (p->contig[q])
+        batch_pass<true><<<p->tiles[q], kThreads, p->smem[q], s>>>(p->items_d[q], p->start_d[q], p->count,
+                                                                   p->ptrs_d, p->ws);
+    else
+        batch_pass<false><<<p->tiles[q], kThreads, p->smem[q], s>>>(p->items_d[q], p->start_d[q], p->count,
+                                                                    p->ptrs_d, p->ws);
+    return cudaGetLastError();
+}
+
+// The dynamic shared-memory limit is an attribute of the kernel, shared by
+// every plan in the process: it only ever rises, so a plan created later with
+// smaller tiles never invalidates an earlier plan's launches.
+cudaError_t raise_smem(bool contig, size_t bytes) {
+    static std::mutex mu;
+    static size_t set[2] = {0, 0};
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& cur = set[contig ? 1 : 0];
+    if (bytes <= cur) return cudaSuccess;
+    const cudaError_t e = contig
+        ? cudaFuncSetAttribute(batch_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes)
+        : cudaFuncSetAttribute(batch_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
+
+cudaError_t upload_pass(chz_batch_plan* p, int q, const std::vector<BatchItem>& items, const std::vector<int>& start) {
+    cudaError_t e = cudaMemcpy(p->items_d[q], items.data(), sizeof(BatchItem) * p->count, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(p->start_d[q], start.data(), sizeof(int) * (p->count + 1), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = raise_smem(p->contig[q], p->smem[q]);
+    return e;
+}
+
+// Autotuner: for every pass, times one launch over all problems at each tile
+// size of kTargets (after a warm-up launch, CUDA events on a private stream)
+// and keeps the fastest.  The launches run on scratch stand-ins for the
+// problems' arrays (zeros; the Neumann data read as zeros), so the caller's
+// data is not needed.  Returns false when the scratch cannot be allocated (the
+// default tile size then stays).
+bool autotune(chz_batch_plan* p, const std::vector<PassTemplate>* tmpl, const std::vector<long long>& ws_off,
+              size_t face_max) {
+    double* fake = nullptr;
+    double* zface = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    bool ok = cudaMalloc(&fake, p->ws_bytes) == cudaSuccess &&
+              cudaMalloc(&zface, face_max * sizeof(double)) == cudaSuccess &&
+              cudaMemset(fake, 0, p->ws_bytes) == cudaSuccess &&
+              cudaMemset(zface, 0, face_max * sizeof(double)) == cudaSuccess &&
+              cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess;
+    if (ok && !p->graph_stream) ok = cudaStreamCreateWithFlags(&p->graph_stream, cudaStreamNonBlocking) == cudaSuccess;
+    if (ok) {
+        for (int i = 0; i < p->count; ++i) {
+            p->ptrs_h[i].f = fake + ws_off[i];
+            for (int k = 0; k < 6; ++k) p->ptrs_h[i].face[k] = zface;
+        }
+        ok = cudaMemcpy(p->ptrs_d, p->ptrs_h, sizeof(ProbPtrs) * p->count, cudaMemcpyHostToDevice) == cudaSuccess;
+    }
+    cudaStream_t s = p->graph_stream;
+    for (int q = 0; ok && q < kPasses; ++q) {
+        float best = 0.0f;
+        int best_t = kDefaultTarget;
+        for (int target : kTargets) {
+            std::vector<BatchItem> items;
+            std::vector<int> start;
+            materialise(tmpl[q], p->contig[q], target, items, start, &p->tiles[q], &p->smem[q]);
+            float ms = 0.0f;
+            ok = upload_pass(p, q, items, start) == cudaSuccess && launch_pass(p, q, s) == cudaSuccess &&
+                 cudaEventRecord(e0, s) == cudaSuccess && launch_pass(p, q, s) == cudaSuccess &&
+                 launch_pass(p, q, s) == cudaSuccess && cudaEventRecord(e1, s) == cudaSuccess &&
+                 cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+            if (!ok) break;
+            if (best == 0.0f || ms < best) {
+                best = ms;
+                best_t = target;
+            }
+        }
+        p->target[q] = best_t;
+        p->tuned_ms[q] = best / 2.0f;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (fake) cudaFree(fake);
+    if (zface) cudaFree(zface);
+    cudaGetLastError();
+    return ok;
+}
+
 // Records the six launches of one batched solve on `s`.
 int enqueue(chz_batch_plan* p, cudaStream_t s) {
     for (int q = 0; q < kPasses; ++q) {
-        if (p->tiles[q] == 0) continue;
-        if (p->contig[q])
-            batch_pass<true><<<p->tiles[q], kThreads, p->smem[q], s>>>(p->items_d[q], p->start_d[q], p->count,
-                                                                       p->ptrs_d, p->ws);
-        else
-            batch_pass<false><<<p->tiles[q], kThreads, p->smem[q], s>>>(p->items_d[q], p->start_d[q], p->count,
-                                                                        p->ptrs_d, p->ws);
-        const cudaError_t e = cudaGetLastError();
+        const cudaError_t e = launch_pass(p, q, s);
         if (e != cudaSuccess) return cuda_fail((int)e, "batched pass");
     }
     batch_fixup<<<p->count, 256, 0, s>>>(p->fix_d, p->ptrs_d);
@@ -211,12 +331,10 @@ int chz_batch_plan_create(int count, const int* dims, const int* bcs, const doub
         p->fix_h[i] = {dims[3 * i], dims[3 * i + 1], dims[3 * i + 2], bcs[3 * i] == 0, bcs[3 * i + 1] == 0,
                        bcs[3 * i + 2] == 0};
     }
-    // descriptors of every pass
-    std::vector<BatchItem> items[kPasses];
-    std::vector<int> start[kPasses];
+    // descriptors of every pass (tile shape chosen below)
+    std::vector<PassTemplate> tmpl[kPasses];
     for (int q = 0; q < kPasses; ++q) {
-        items[q].resize(count);
-        start[q].resize(count + 1);
+        tmpl[q].resize(count);
         p->contig[q] = (q == 0 || q == 4);
     }
     for (int i = 0; i < count; ++i) {
@@ -234,11 +352,11 @@ int chz_batch_plan_create(int count, const int* dims, const int* bcs, const doub
         const long long fy = nx + 1, fz = (long long)(nx + 1) * (ny + 1);
         const long long wy = nx + 2, wz = (long long)(nx + 2) * (ny + 2);
         const double lam = lambdas[i];
-        auto fill = [&](int q, int kind, int kind2, const DeviceLineTables& t, int n, bool contig, int u0, int u1,
-                        int v0, int v1, long long isu, long long isv, long long isl, int ld0, int ld1, long long osu,
-                        long long osv, long long osl, int st0, int st1, int in_user, int out_user) {
-            const LineGeom g = line_geometry(n, 1, contig);
-            BatchItem& it = items[q][i];
+        auto fill = [&](int q, int kind, int kind2, const DeviceLineTables& t, int n, int u0, int u1, int v0, int v1,
+                        long long isu, long long isv, long long isl, int ld0, int ld1, long long osu, long long osv,
+                        long long osl, int st0, int st1, int in_user, int out_user) {
+            PassTemplate& tp = tmpl[q][i];
+            BatchItem& it = tp.it;
             std::memset(&it, 0, sizeof(it));
             PassArgs& a = it.a;
             a.kind = kind; a.kind2 = kind2;
@@ -246,33 +364,30 @@ int chz_batch_plan_create(int count, const int* dims, const int* bcs, const doub
             a.in_su = isu; a.in_sv = isv; a.in_sl = isl; a.ld_lo = ld0; a.ld_hi = ld1;
             a.out_su = osu; a.out_sv = osv; a.out_sl = osl; a.st_lo = st0; a.st_hi = st1;
             a.scale = 1.0; a.use_scale = 0;
-            a.PR = g.PR; a.log2W = g.log2W;
             it.tb.twM = static_cast<const double2*>(t.twM);
             it.tb.twN = static_cast<const double2*>(t.twN);
             it.tb.tw4N = static_cast<const double2*>(t.tw4N);
             it.tb.inv4sin = static_cast<const double*>(t.inv4sin);
             it.tb.N = t.N; it.tb.M = t.M; it.tb.rp = t.rp;
-            it.buf_elems = (int)g.buf_elems;
-            it.ntx = (a.nu + g.W - 1) / g.W;
             it.in_user = in_user; it.out_user = out_user;
             it.ws_off = ws_off[i];
-            start[q][i + 1] = it.ntx * (v1 - v0 + 1);
-            p->smem[q] = std::max(p->smem[q], g.smem_bytes);
+            tp.n = n;
+            tp.nv = v1 - v0 + 1;
         };
-        fill(0, X.kf, -1, tx, nx, true, Y.s, Y.e, Z.s, Z.e, fy, fz, 1, X.s, X.e, wy, wz, 1, X.sp0, X.sp1, 1, 0);
+        fill(0, X.kf, -1, tx, nx, Y.s, Y.e, Z.s, Z.e, fy, fz, 1, X.s, X.e, wy, wz, 1, X.sp0, X.sp1, 1, 0);
         {
-            BcArgs& bc = items[0][i].a.bc;
-            items[0][i].a.has_bc = 1;
+            BcArgs& bc = tmpl[0][i].it.a.bc;
+            tmpl[0][i].it.a.has_bc = 1;
             bc.xbc = X.bc; bc.ybc = Y.bc; bc.zbc = Z.bc;
             bc.xs = X.s; bc.xe = X.e; bc.ys = Y.s; bc.ye = Y.e; bc.zs = Z.s; bc.ze = Z.e;
             bc.nx = nx; bc.ny = ny; bc.nz = nz;
             bc.dx = X.d; bc.dy = Y.d; bc.dz = Z.d;
             bc.dx2 = X.d2; bc.dy2 = Y.d2; bc.dz2 = Z.d2;
         }
-        fill(1, Y.kf, -1, ty, ny, false, X.sp0, X.sp1, Z.s, Z.e, 1, wz, wy, Y.s, Y.e, 1, wz, wy, Y.sp0, Y.sp1, 0, 0);
-        fill(2, Z.kf, Z.ki, tz, nz, false, X.sp0, X.sp1, Y.sp0, Y.sp1, 1, wy, wz, Z.s, Z.e, 1, wy, wz, Z.s, Z.e, 0, 0);
+        fill(1, Y.kf, -1, ty, ny, X.sp0, X.sp1, Z.s, Z.e, 1, wz, wy, Y.s, Y.e, 1, wz, wy, Y.sp0, Y.sp1, 0, 0);
+        fill(2, Z.kf, Z.ki, tz, nz, X.sp0, X.sp1, Y.sp0, Y.sp1, 1, wy, wz, Z.s, Z.e, 1, wy, wz, Z.s, Z.e, 0, 0);
         {
-            PassArgs& a = items[2][i].a;
+            PassArgs& a = tmpl[2][i].it.a;
             a.has_div = 1;
             a.dv.ex = ex; a.dv.ey = ey; a.dv.ez = ez;
             a.dv.lambda = lam;
@@ -283,15 +398,16 @@ int chz_batch_plan_create(int count, const int* dims, const int* bcs, const doub
             a.dv.zz_hi = Z.bc == 0 ? 1 : 0;
             a.dv.lo = Z.sp0; a.dv.hi = Z.sp1;
         }
-        fill(3, Y.ki, -1, ty, ny, false, X.sp0, X.sp1, Z.s, Z.e, 1, wz, wy, Y.sp0, Y.sp1, 1, wz, wy, Y.s, Y.e, 0, 0);
-        fill(4, X.ki, -1, tx, nx, true, Y.s, Y.e, Z.s, Z.e, wy, wz, 1, X.sp0, X.sp1, fy, fz, 1, X.s, X.e, 0, 1);
-        items[4][i].a.scale = solver_scale(X, Y, Z);
-        items[4][i].a.use_scale = 1;
+        fill(3, Y.ki, -1, ty, ny, X.sp0, X.sp1, Z.s, Z.e, 1, wz, wy, Y.sp0, Y.sp1, 1, wz, wy, Y.s, Y.e, 0, 0);
+        fill(4, X.ki, -1, tx, nx, Y.s, Y.e, Z.s, Z.e, wy, wz, 1, X.sp0, X.sp1, fy, fz, 1, X.s, X.e, 0, 1);
+        tmpl[4][i].it.a.scale = solver_scale(X, Y, Z);
+        tmpl[4][i].it.a.use_scale = 1;
     }
+    std::vector<BatchItem> items[kPasses];
+    std::vector<int> start[kPasses];
     for (int q = 0; q < kPasses; ++q) {
-        start[q][0] = 0;
-        for (int i = 0; i < count; ++i) start[q][i + 1] += start[q][i];
-        p->tiles[q] = start[q][count];
+        p->target[q] = kDefaultTarget;
+        materialise(tmpl[q], p->contig[q], p->target[q], items[q], start[q], &p->tiles[q], &p->smem[q]);
     }
     // device copies, workspace, pinned pointer table
     cudaError_t e = cudaSuccess;
@@ -309,13 +425,22 @@ int chz_batch_plan_create(int count, const int* dims, const int* bcs, const doub
     if (e == cudaSuccess) e = cudaMallocHost(&p->ptrs_h, sizeof(ProbPtrs) * count);
     p->ws_bytes = (size_t)ws_total * sizeof(double);
     if (e == cudaSuccess) e = cudaMalloc(&p->ws, p->ws_bytes);
-    if (e == cudaSuccess) {
-        // one attribute per kernel instantiation: the largest need of its passes
-        size_t sc = 0, ss = 0;
-        for (int q = 0; q < kPasses; ++q) (p->contig[q] ? sc : ss) = std::max(p->contig[q] ? sc : ss, p->smem[q]);
-        e = cudaFuncSetAttribute(batch_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(batch_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss);
+    if (e == cudaSuccess && g_autotune.load(std::memory_order_relaxed)) {
+        size_t face_max = 1;
+        for (int i = 0; i < count; ++i) {
+            const size_t nx = dims[3 * i], ny = dims[3 * i + 1], nz = dims[3 * i + 2];
+            face_max = std::max(face_max, std::max((ny + 1) * (nz + 1), std::max((nx + 1) * (nz + 1), (nx + 1) * (ny + 1))));
+        }
+        if (!autotune(p, tmpl, ws_off, face_max)) {
+            for (int q = 0; q < kPasses; ++q) {
+                p->target[q] = kDefaultTarget;
+                p->tuned_ms[q] = 0.0f;
+            }
+        }
+    }
+    for (int q = 0; q < kPasses && e == cudaSuccess; ++q) {
+        materialise(tmpl[q], p->contig[q], p->target[q], items[q], start[q], &p->tiles[q], &p->smem[q]);
+        e = upload_pass(p, q, items[q], start[q]);
     }
     if (e != cudaSuccess) {
         const int st = (e == cudaErrorMemoryAllocation) ? fail(CHZ_ERROR_ALLOC, "batch plan allocation failed")
@@ -328,6 +453,17 @@ int chz_batch_plan_create(int count, const int* dims, const int* bcs, const doub
 }
 
 size_t chz_batch_workspace_bytes(const chz_batch_plan* plan) { return plan ? plan->ws_bytes : 0; }
+
+int chz_batch_set_autotune(int on) { return g_autotune.exchange(on ? 1 : 0); }
+
+int chz_batch_plan_tiles(const chz_batch_plan* plan, int* targets, float* ms) {
+    if (!plan) return fail(CHZ_ERROR_INVALID_VALUE, "NULL plan");
+    for (int q = 0; q < kPasses; ++q) {
+        if (targets) targets[q] = plan->target[q];
+        if (ms) ms[q] = plan->tuned_ms[q];
+    }
+    return CHZ_SUCCESS;
+}
 
 int chz_batch_solve(chz_batch_plan* p, double* const* f, const double* const* faces, void* stream) {
     g_last_error[0] = 0;

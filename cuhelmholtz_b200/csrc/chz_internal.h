@@ -119,6 +119,10 @@ int get_line_tables(int N, int is_double, int device, DeviceLineTables* out);
 int factor_radices(int M, RadixPlan* rp);
 bool radix_plan_is_pow2(const RadixPlan& rp);
 LineGeom line_geometry(int N, int is_double, bool contig);
+// The same with an explicit tile size: W = the largest power of two with
+// W * N <= target (2 <= W <= 64), halved while the shared memory would exceed
+// `max_smem` bytes.
+LineGeom line_geometry_target(int N, int is_double, bool contig, int target, size_t max_smem);
 
 // Launchers (return cudaError_t as int).
 enum IoType { kIoF64 = 0, kIoF32 = 1 };

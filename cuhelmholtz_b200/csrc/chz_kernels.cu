@@ -117,12 +117,22 @@ bool radix_plan_is_pow2(const RadixPlan& rp) {
 static int ilog2(int x) { int r = 0; while ((1 << (r + 1)) <= x) ++r; return r; }
 
 LineGeom line_geometry(int N, int is_double, bool contig) {
+    return line_geometry_target(N, is_double, contig, is_double ? 4096 : 8192, ~(size_t)0);
+}
+
+LineGeom line_geometry_target(int N, int is_double, bool contig, int target, size_t max_smem) {
     LineGeom g{};
     g.N = N;
     g.M = N / 2;
-    const int target = is_double ? 4096 : 8192;
     int W = 1 << ilog2(std::max(1, target / N));
     W = std::max(2, std::min(64, W));
+    const size_t esz0 = is_double ? 8 : 4;
+    while (W > 2) {
+        const size_t pr = contig ? W + 1 : W;
+        const size_t be = ((std::max(((size_t)N + 2) * pr, (size_t)N * W) + 3) & ~(size_t)3);
+        if ((2 * be + kThreads + W) * esz0 <= max_smem) break;
+        W >>= 1;
+    }
     g.W = W;
     g.log2W = ilog2(W);
     g.PR = contig ? W + 1 : W;

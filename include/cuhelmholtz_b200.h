@@ -138,6 +138,16 @@ int chz_batch_solve(chz_batch_plan* plan, double* const* f, const double* const*
 size_t chz_batch_workspace_bytes(const chz_batch_plan* plan);
 int chz_batch_plan_destroy(chz_batch_plan* plan);
 
+/* Autotuner of the batch plans (on by default): chz_batch_plan_create times
+ * every pass over all problems at tile sizes of 1024..16384 values per tile,
+ * on scratch stand-ins for the problems' arrays, and keeps the fastest per
+ * pass.  Returns the previous setting. */
+int chz_batch_set_autotune(int on);
+
+/* Tile size chosen for each of the five passes (values per tile; targets[5])
+ * and its measured time per launch in ms (ms[5]; 0 when not tuned). */
+int chz_batch_plan_tiles(const chz_batch_plan* plan, int* targets, float* ms);
+
 /* Helmholtz solve with FP32 transforms and FP64 iterative refinement.
  * u0 = S32(b); then up to max_corrections times: r = b - A u in FP64 (the
  * 7-point operator with the boundary terms, as the FP64 solve's system),

@@ -83,3 +83,30 @@ def test_batch_rejects_bad_plans():
         api.BatchPlan([dict(nx=8, ny=8, nz=8, xbc=5, ybc=1, zbc=1, lam=-1.0)])
     with pytest.raises(api.CHZError):
         api.BatchPlan([dict(nx=7, ny=8, nz=8, xbc=1, ybc=1, zbc=1, lam=-1.0)])
+
+
+def test_autotuned_and_default_tiles_agree():
+    """The autotuner picks a tile size per pass among 1024..16384 values per
+    tile; the tuned plan and the untuned (4096 everywhere) plan give the same
+    solves (1e-13), and both match single solves (1e-12)."""
+    probs = gen.config4_problems(count=16, seed=13)
+    tuned = api.BatchPlan(probs)
+    targets, ms = tuned.tiles()
+    assert all(t in (1024, 2048, 4096, 8192, 16384) for t in targets), targets
+    assert all(m > 0 for m in ms), ms
+    prev = api.BatchPlan.set_autotune(False)
+    try:
+        plain = api.BatchPlan(probs)
+    finally:
+        api.BatchPlan.set_autotune(prev)
+    t2, ms2 = plain.tiles()
+    assert t2 == [4096] * 5 and ms2 == [0.0] * 5
+    a = [_dev(p) for p in probs]
+    b = [_dev(p) for p in probs]
+    tuned.solve([d[0] for d in a], [d[1] for d in a])
+    plain.solve([d[0] for d in b], [d[1] for d in b])
+    torch.cuda.synchronize()
+    for p, da, db in zip(probs, a, b):
+        ua, ub = da[0].cpu().numpy(), db[0].cpu().numpy()
+        assert _rel(ua, ub) < 1e-13
+        assert _rel(ua, _single(p)) < 1e-12
