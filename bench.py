@@ -385,10 +385,16 @@ def run_ours(args):
         torch.cuda.synchronize()
         rel_err = float((torch.linalg.vector_norm(a32 - a64) / torch.linalg.vector_norm(a64)).item())
         del a64, a32
+        # per-kernel times of one refined solve (event tracing)
+        _lib.trace_enable(True)
+        solve_refined(fs[0])
+        torch.cuda.synchronize()
+        _lib.trace_enable(False)
+        rtr = {k: {"launches": v[0], "avg_ms": v[1] / v[0]} for k, v in _lib.trace_collect().items()}
         rbytes = (48 + 72 * K) * nx * ny * nz
         refine = {"value": rvalue, "unit": "solves/s", "corrections": K,
                   "rel_err_vs_fp64": rel_err, "speedup_vs_fp64": rvalue / value,
-                  "model_bytes_per_solve": rbytes,
+                  "model_bytes_per_solve": rbytes, "per_kernel": rtr,
                   "hbm_gbs_model": rbytes * rvalue / world / 1e9}
 
     # ---- end to end through the public API with host buffers ----

@@ -561,8 +561,37 @@ fast_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tg, int ntx, int ntil
             const long long vb = (long long)v * a.out_sv;
             const double sc = a.use_scale ? a.scale : 1.0;
             if constexpr (CONTIG) {
+                // accumulated output (the refinement's update u += c): all of
+                // a thread's u values are loaded before any store, so the
+                // loads overlap instead of one latency per row
+                constexpr int NI = (N + 2 + kNT - 1) / kNT;
+                bool done = false;
+                if constexpr (W * NI <= 48) {
+                    if (a.acc) {
+                        double av[W][NI];
+#pragma unroll
+                        for (int cc = 0; cc < W; ++cc) {
+                            const double* arow = a.acc + vb + (long long)(ub + cc) * a.out_su;
+#pragma unroll
+                            for (int it = 0; it < NI; ++it) {
+                                const int l = lo + t + it * kNT;
+                                av[cc][it] = (cc < nl && l <= hi) ? __ldg(arow + l) : 0.0;
+                            }
+                        }
+#pragma unroll
+                        for (int cc = 0; cc < W; ++cc) {
+                            TO* row = out + vb + (long long)(ub + cc) * a.out_su;
+#pragma unroll
+                            for (int it = 0; it < NI; ++it) {
+                                const int l = lo + t + it * kNT;
+                                if (cc < nl && l <= hi) row[l] = (TO)(av[cc][it] + (double)buf[l * PR + cc] * sc);
+                            }
+                        }
+                        done = true;
+                    }
+                }
 #pragma unroll 1
-                for (int cc = 0; cc < nl; ++cc) {
+                for (int cc = 0; cc < (done ? 0 : nl); ++cc) {
                     const long long ro = vb + (long long)(ub + cc) * a.out_su;
                     TO* row = out + ro;
                     if (a.acc) {

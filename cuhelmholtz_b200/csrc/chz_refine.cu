@@ -96,59 +96,93 @@ __global__ void remove_mode(double* u, BcArgs b, const double* sum, double inv_w
 // r = b - A u at the unknown nodes, with A's homogeneous closures: Dirichlet
 // neighbours are 0 (their values are in b), a Neumann ghost mirrors the
 // interior neighbour (the flux is in b), periodic neighbours wrap.
-__global__ void residual_kernel(ResidualArgs a) {
-    const BcArgs& b = a.bc;
-    const int i = b.xs + blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = b.ys + blockIdx.y;
-    const int k = b.zs + blockIdx.z;
-    double r2 = 0.0, b2 = 0.0;
-    if (i <= b.xe) {
-        const long long sy = b.nx + 1, sz = (long long)(b.nx + 1) * (b.ny + 1);
-        const long long o = k * sz + j * sy + i;
-        const double* u = a.u;
-        const double uc = u[o];
-        // x neighbours
-        double ul, ur;
-        if (i == b.xs) {
-            ul = (b.xbc == 0) ? u[o - i + (b.nx - 1)] : (b.xbc >= 3 ? u[o + 1] : 0.0);
-        } else {
-            ul = u[o - 1];
-        }
-        if (i == b.xe) {
-            ur = (b.xbc == 0) ? u[o - i] : ((b.xbc == 2 || b.xbc == 3) ? u[o - 1] : 0.0);
-        } else {
-            ur = u[o + 1];
-        }
-        double dl, dr;
-        if (j == b.ys) {
-            dl = (b.ybc == 0) ? u[o + (b.ny - 1 - j) * sy] : (b.ybc >= 3 ? u[o + sy] : 0.0);
-        } else {
-            dl = u[o - sy];
-        }
-        if (j == b.ye) {
-            dr = (b.ybc == 0) ? u[o - j * sy] : ((b.ybc == 2 || b.ybc == 3) ? u[o - sy] : 0.0);
-        } else {
-            dr = u[o + sy];
-        }
-        double fl, fr;
-        if (k == b.zs) {
-            fl = (b.zbc == 0) ? u[o + (long long)(b.nz - 1 - k) * sz] : (b.zbc >= 3 ? u[o + sz] : 0.0);
-        } else {
-            fl = u[o - sz];
-        }
-        if (k == b.ze) {
-            fr = (b.zbc == 0) ? u[o - (long long)k * sz] : ((b.zbc == 2 || b.zbc == 3) ? u[o - sz] : 0.0);
-        } else {
-            fr = u[o + sz];
-        }
-        const double au = (((ul - 2.0 * uc + ur) * b.dx2 + (dl - 2.0 * uc + dr) * b.dy2) +
-                           (fl - 2.0 * uc + fr) * b.dz2) + a.lambda * uc;
-        const double bv = bc_terms(__ldg(b.f + o), b, i, j, k);
-        const double rv = a.shift ? (bv - au) - *a.shift * a.inv_w : bv - au;
-        a.r[k * a.rz + j * a.ry + i] = (float)rv;
-        r2 = rv * rv;
-        b2 = bv * bv;
+//
+// A block of 32 x 8 threads marches up kResZ planes of a 32 x 8 column.  The u
+// values of each plane, with a one-point halo, are staged in shared memory by
+// cp.async, two planes ahead of the plane being computed (a ring of four
+// plane tiles); the closures are folded into the halo values as they are
+// loaded, so the stencil itself reads only shared memory.
+constexpr int kResX = 32, kResY = 8, kResZ = 32;
+constexpr int kHX = kResX + 2, kHY = kResY + 2, kHalo = kHX * kHY;
+
+// Source index along one axis for window-relative neighbour g (one step
+// outside the window at most): -1 when the value is 0 (Dirichlet neighbour).
+__device__ __forceinline__ int closure_index(int g, int s, int e, int n, int bc) {
+    if (g >= s && g <= e) return g;
+    if (g == s - 1) {
+        if (bc == 0) return n - 1;          // periodic: s = 0
+        if (bc == 3 || bc == 4) return s + 1;  // Neumann mirror
+        return -1;                          // Dirichlet
     }
+    if (g == e + 1) {
+        if (bc == 0) return 0;
+        if (bc == 2 || bc == 3) return e - 1;
+        return -1;
+    }
+    return -1;  // beyond the halo: never read
+}
+
+__device__ __forceinline__ void load_plane(double* tile, const double* u, const BcArgs& b, int i0, int j0, int p,
+                                           long long sy, long long sz, int tid) {
+    const int kk = closure_index(p, b.zs, b.ze, b.nz, b.zbc);
+    for (int e = tid; e < kHalo; e += kResX * kResY) {
+        const int hy = e / kHX, hx = e - hy * kHX;
+        const int ii = closure_index(i0 - 1 + hx, b.xs, b.xe, b.nx, b.xbc);
+        const int jj = closure_index(j0 - 1 + hy, b.ys, b.ye, b.ny, b.ybc);
+        const bool valid = kk >= 0 && ii >= 0 && jj >= 0;
+        const double* src = valid ? u + (long long)kk * sz + (long long)jj * sy + ii : u;
+        cp_async_elem<8>(tile + e, src, valid);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+__global__ void __launch_bounds__(kResX * kResY) residual_kernel(ResidualArgs a) {
+    __shared__ __align__(16) double ring[4][kHalo];
+    const BcArgs& b = a.bc;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kResX + tx;
+    const int i0 = b.xs + blockIdx.x * kResX, j0 = b.ys + blockIdx.y * kResY;
+    const int i = i0 + tx, j = j0 + ty;
+    const int k0 = b.zs + blockIdx.z * kResZ;
+    const int k1 = min(k0 + kResZ - 1, b.ze);
+    const long long sy = b.nx + 1, sz = (long long)(b.nx + 1) * (b.ny + 1);
+    const bool act = i <= b.xe && j <= b.ye;
+    const bool side = (i == b.xs || i == b.xe || j == b.ys || j == b.ye);
+    const double shift = a.shift ? *a.shift * a.inv_w : 0.0;
+    double r2 = 0.0, b2 = 0.0;
+    // planes k0 - 1, k0, k0 + 1 and (prefetch) k0 + 2 in slots 0..3
+    for (int q = 0; q < 4; ++q) {
+        if (k0 - 1 + q <= k1 + 1) load_plane(ring[q], a.u, b, i0, j0, k0 - 1 + q, sy, sz, tid);
+        else asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
+    const double* fcol = b.f + (long long)j * sy + i;
+    double fv = act ? __ldg(fcol + (long long)k0 * sz) : 0.0;
+    const int c = (ty + 1) * kHX + tx + 1;
+    for (int k = k0; k <= k1; ++k) {
+        const int q = k - k0;  // slot of plane k - 1 is q & 3
+        // planes k - 1, k, k + 1 have landed (plane k + 2 may still be in flight)
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        __syncthreads();
+        const double fnext = (act && k + 1 <= k1) ? __ldg(fcol + (long long)(k + 1) * sz) : 0.0;
+        if (act) {
+            const double* lo = ring[q & 3];
+            const double* mid = ring[(q + 1) & 3];
+            const double* hi = ring[(q + 2) & 3];
+            const double uc = mid[c];
+            const double au = (((mid[c - 1] - 2.0 * uc + mid[c + 1]) * b.dx2 +
+                                (mid[c - kHX] - 2.0 * uc + mid[c + kHX]) * b.dy2) +
+                               (lo[c] - 2.0 * uc + hi[c]) * b.dz2) + a.lambda * uc;
+            const double bv = (side || k == b.zs || k == b.ze) ? bc_terms(fv, b, i, j, k) : fv;
+            const double rv = (bv - au) - shift;
+            a.r[k * a.rz + j * a.ry + i] = (float)rv;
+            r2 += rv * rv;
+            b2 += bv * bv;
+        }
+        fv = fnext;
+        __syncthreads();  // slot of plane k - 1 is free
+        if (k + 3 <= k1 + 1) load_plane(ring[q & 3], a.u, b, i0, j0, k + 3, sy, sz, tid);
+        else asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     if (a.sums) {
         // block reduction, then one atomic per block
         __shared__ double s0[32], s1[32];
@@ -157,14 +191,15 @@ __global__ void residual_kernel(ResidualArgs a) {
             r2 += __shfl_down_sync(0xffffffffu, r2, off);
             b2 += __shfl_down_sync(0xffffffffu, b2, off);
         }
-        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        const int t = threadIdx.y * kResX + threadIdx.x;
+        const int lane = t & 31, wid = t >> 5;
         if (lane == 0) {
             s0[wid] = r2;
             s1[wid] = b2;
         }
         __syncthreads();
         if (wid == 0) {
-            const int nw = blockDim.x >> 5;
+            constexpr int nw = kResX * kResY / 32;
             r2 = lane < nw ? s0[lane] : 0.0;
             b2 = lane < nw ? s1[lane] : 0.0;
 #pragma unroll
@@ -360,6 +395,8 @@ extern "C" int chz_helmholtz_solve_refined(double left, double right, int nx, in
         if ((rc = solve32_passes(X, Y, Z, tx, ty, tz, ex, ey, ez, lambda, &bc, f, w, u, nullptr, s))) return rc;
         const dim3 rblock(128, 1, 1);
         const dim3 rgrid((X.e - X.s + 1 + 127) / 128, Y.e - Y.s + 1, Z.e - Z.s + 1);
+        const dim3 resblock(kResX, kResY, 1);  // planes per block: kResZ
+        const dim3 resgrid((X.e - X.s + kResX) / kResX, (Y.e - Y.s + kResY) / kResY, (Z.e - Z.s + kResZ) / kResZ);
         if (singular) {
             cudaError_t e = cudaMemsetAsync(sums + 2, 0, 2 * sizeof(double), s);
             if (e != cudaSuccess) return cuda_fail((int)e, "memset");
@@ -384,7 +421,7 @@ extern "C" int chz_helmholtz_solve_refined(double left, double right, int nx, in
                 if (e != cudaSuccess) return cuda_fail((int)e, "memset");
             }
             trace_begin(s, "refine_residual");
-            residual_kernel<<<rgrid, rblock, 0, s>>>(ra);
+            residual_kernel<<<resgrid, resblock, 0, s>>>(ra);
             count_launch();
             trace_end(s);
             cudaError_t e = cudaGetLastError();
