@@ -238,6 +238,27 @@ def run_reference_arm(args):
 
 
 # ---------------------------------------------------------------------------
+# multi-rank bookkeeping (one process per GPU, independent replicas)
+# ---------------------------------------------------------------------------
+
+def max_over_ranks(ms, world, device):
+    """The largest of the ranks' device times (every rank calls this, in the
+    same order; a single process returns its own)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(units_per_rank, max_ms):
+    """Whole-job units per second: all ranks' units over the slowest rank's
+    time."""
+    return units_per_rank / (max_ms / 1000.0)
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 
@@ -316,12 +337,9 @@ def run_ours(args):
     elapsed_ms = ev0.elapsed_time(ev1)
     clocks = sampler.stop() if sampler else None
     barrier()
-    t = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    elapsed_max_ms = float(t.item())
+    elapsed_max_ms = max_over_ranks(elapsed_ms, world, "cuda")
     solves = world * args.steps * B
-    value = solves / (elapsed_max_ms / 1000.0)
+    value = job_throughput(solves, elapsed_max_ms)
     ms_per_step = elapsed_max_ms / args.steps
 
     # ---- per-kernel times with CUDA events on the launching stream ----
@@ -373,10 +391,7 @@ def run_ours(args):
                 solve_refined(f)
         r1.record(stream)
         torch.cuda.synchronize()
-        t = torch.tensor([r0.elapsed_time(r1)], device="cuda", dtype=torch.float64)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        rvalue = world * args.steps * B / (float(t.item()) / 1000.0)
+        rvalue = job_throughput(world * args.steps * B, max_over_ranks(r0.elapsed_time(r1), world, "cuda"))
         # accuracy on the benchmark problem: refined vs FP64 solve of the same input
         a64 = f_host.to("cuda")
         a32 = f_host.to("cuda")
@@ -415,10 +430,7 @@ def run_ours(args):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * esteps / (float(t.item()) / 1000.0)
+    e2e_value = job_throughput(world * esteps, max_over_ranks(e2e_ms, world, "cuda"))
 
     # ---- accuracy of the benchmarked solve: relative residual (FP64, host) ----
     rel_residual = None
