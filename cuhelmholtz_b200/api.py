@@ -120,6 +120,29 @@ def cuda_helmholtz_solver(left, right, NX, xbc, bcl, bcr,
     return 0
 
 
+def helmholtz_solve_pertrb(left, right, NX, xbc, bcl, bcr,
+                           bottom, top, NY, ybc, bcb, bct,
+                           front, back, NZ, zbc, bcf, bce,
+                           lambda_, f, stream=None) -> float:
+    """cuda_helmholtz_solver that also returns FISHPACK's PERTRB: for a
+    singular problem (lambda = 0, every code 0 or 3) the constant removed from
+    the right-hand side so that a solution exists, else 0.  Solves in place
+    on ``f`` (the zero-mode solution)."""
+    import ctypes
+    n = (NX + 1) * (NY + 1) * (NZ + 1)
+    pf = _ptr(f, "f", n)
+    fx, fy, fz = (_face_len(a, NX, NY, NZ) for a in "xyz")
+    faces = [_ptr(bcl, "bcl", fx), _ptr(bcr, "bcr", fx), _ptr(bcb, "bcb", fy),
+             _ptr(bct, "bct", fy), _ptr(bcf, "bcf", fz), _ptr(bce, "bce", fz)]
+    out = ctypes.c_double(0.0)
+    _check(_lib.lib().chz_helmholtz_solve_pertrb(
+        float(left), float(right), NX, xbc, faces[0], faces[1],
+        float(bottom), float(top), NY, ybc, faces[2], faces[3],
+        float(front), float(back), NZ, zbc, faces[4], faces[5],
+        float(lambda_), pf, ctypes.byref(out), _stream(stream)))
+    return out.value
+
+
 def helmholtz_solve_refined(left, right, NX, xbc, bcl, bcr,
                             bottom, top, NY, ybc, bcb, bct,
                             front, back, NZ, zbc, bcf, bce,

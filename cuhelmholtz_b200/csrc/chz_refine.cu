@@ -1,4 +1,5 @@
-// FP32 transforms with FP64 iterative refinement: chz_helmholtz_solve_refined.
+// FP32 transforms with FP64 iterative refinement: chz_helmholtz_solve_refined;
+// and the solve with FISHPACK's PERTRB, chz_helmholtz_solve_pertrb (end of file).
 //
 // The system is the reference's (cuda_helmholtz_solver.cu:33-380): A u = b on
 // the unknown windows, b = f with the boundary terms of _3d_bc*_ini_*
@@ -463,4 +464,62 @@ extern "C" int chz_helmholtz_solve_refined(double left, double right, int nx, in
     if (corrections_done) *corrections_done = done;
     if (rel_residual) *rel_residual = last_rel;
     return CHZ_SUCCESS;
+}
+
+// Solve with FISHPACK's PERTRB (the constant hw3crt subtracts from the
+// right-hand side of a singular problem so that a solution exists).  The
+// diagonal solve already removes the constant mode, which solves the system
+// with b - PERTRB, so the solution is the plain solve's; PERTRB itself is the
+// weighted mean 1^T W b / 1^T W 1 over the unknown window (mode_sum), read
+// back before the solve overwrites f.
+extern "C" int chz_helmholtz_solve_pertrb(double left, double right, int nx, int xbc, const double* bcl,
+                                          const double* bcr, double bottom, double top, int ny, int ybc,
+                                          const double* bcb, const double* bct, double front, double back, int nz,
+                                          int zbc, const double* bcf, const double* bce, double lambda, double* f,
+                                          double* pertrb, void* stream) {
+    g_last_error[0] = 0;
+    if (!pertrb) return fail(CHZ_ERROR_INVALID_VALUE, "pertrb is NULL");
+    *pertrb = 0.0;
+    int rc;
+    AxisSolve X, Y, Z;
+    if ((rc = setup_axis(nx, xbc, left, right, &X)) || (rc = setup_axis(ny, ybc, bottom, top, &Y)) ||
+        (rc = setup_axis(nz, zbc, front, back, &Z)))
+        return rc;
+    const bool singular = lambda == 0.0 && (X.bc == 0 || X.bc == 3) && (Y.bc == 0 || Y.bc == 3) &&
+                          (Z.bc == 0 || Z.bc == 3);
+    if (!singular)
+        return chz_helmholtz_solve(left, right, nx, xbc, bcl, bcr, bottom, top, ny, ybc, bcb, bct, front, back, nz,
+                                   zbc, bcf, bce, lambda, f, stream);
+    if ((rc = check_len(nx, "x")) || (rc = check_len(ny, "y")) || (rc = check_len(nz, "z"))) return rc;
+    if (!f) return fail(CHZ_ERROR_INVALID_VALUE, "f is NULL");
+    if ((rc = check_faces(X, bcl, bcr, "x")) || (rc = check_faces(Y, bcb, bct, "y")) ||
+        (rc = check_faces(Z, bcf, bce, "z")))
+        return rc;
+    const size_t need = chz_helmholtz_workspace_size(nx, ny, nz, 0);
+    void* ws = nullptr;
+    if ((rc = cached_workspace(stream, need + 256, &ws))) return rc;
+    double* acc = reinterpret_cast<double*>(static_cast<char*>(ws) + need);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    BcArgs bc{};
+    bc.xbc = X.bc; bc.ybc = Y.bc; bc.zbc = Z.bc;
+    bc.xs = X.s; bc.xe = X.e; bc.ys = Y.s; bc.ye = Y.e; bc.zs = Z.s; bc.ze = Z.e;
+    bc.nx = nx; bc.ny = ny; bc.nz = nz;
+    bc.dx = X.d; bc.dy = Y.d; bc.dz = Z.d;
+    bc.dx2 = X.d2; bc.dy2 = Y.d2; bc.dz2 = Z.d2;
+    bc.f = f;
+    bc.bcl = bcl; bc.bcr = bcr; bc.bcb = bcb; bc.bct = bct; bc.bcf = bcf; bc.bce = bce;
+    cudaError_t e = cudaMemsetAsync(acc, 0, sizeof(double), s);
+    if (e != cudaSuccess) return cuda_fail((int)e, "memset");
+    const dim3 block(128, 1, 1);
+    const dim3 grid((X.e - X.s + 1 + 127) / 128, Y.e - Y.s + 1, Z.e - Z.s + 1);
+    mode_sum<<<grid, block, 0, s>>>(bc, nullptr, acc);
+    count_launch();
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail((int)e, "weighted mean");
+    double h = 0.0;
+    e = cudaMemcpyAsync(&h, acc, sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail((int)e, "weighted mean read-back");
+    *pertrb = h / ((double)nx * (double)ny * (double)nz);  // 1^T W 1 over the window
+    return chz_helmholtz_solve_ws(left, right, nx, xbc, bcl, bcr, bottom, top, ny, ybc, bcb, bct, front, back, nz,
+                                  zbc, bcf, bce, lambda, f, ws, need, stream);
 }

@@ -84,6 +84,24 @@ int chz_helmholtz_solve(double left, double right, int nx, int xbc,
 
 /* As chz_helmholtz_solve with a caller-owned device workspace of at least
  * chz_helmholtz_workspace_size(nx, ny, nz, 0) bytes, 256-byte aligned. */
+/* Helmholtz solve as chz_helmholtz_solve that also returns PERTRB, as
+ * FISHPACK's hw3crt does (hw3crt_wrapper.cpp:20-28 passes &pertrb to hw3crt_
+ * but does not return it): when lambda = 0 and every code is 0 or 3 the
+ * problem is singular and PERTRB is the constant removed from the right-hand
+ * side so that a solution exists -- the weighted mean of b (f with the
+ * boundary terms) over the unknown window, weight 1/2 per Neumann boundary
+ * index; otherwise 0.  The solution is chz_helmholtz_solve's (its constant
+ * mode is 0; hw3crt returns the same solution plus an arbitrary constant).
+ * *pertrb is a host value; in the singular case the call waits for `stream`
+ * to read it back. */
+int chz_helmholtz_solve_pertrb(double left, double right, int nx, int xbc,
+                               const double* bcl, const double* bcr,
+                               double bottom, double top, int ny, int ybc,
+                               const double* bcb, const double* bct,
+                               double front, double back, int nz, int zbc,
+                               const double* bcf, const double* bce,
+                               double lambda, double* f, double* pertrb, void* stream);
+
 int chz_helmholtz_solve_ws(double left, double right, int nx, int xbc,
                            const double* bcl, const double* bcr,
                            double bottom, double top, int ny, int ybc,

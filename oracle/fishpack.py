@@ -67,6 +67,27 @@ def solve(p, repeats=1, timeout=3600):
     return u, best, med
 
 
+def solve_with_pertrb(p, timeout=600):
+    """Calls hw3crt directly (not through the wrapper, which drops PERTRB)
+    and returns (u, pertrb, ierror)."""
+    if not available():
+        raise RuntimeError(f"fishpack runner not built: {BINARY} (run make -C oracle)")
+    with tempfile.TemporaryDirectory() as td:
+        fin = os.path.join(td, "in.bin")
+        fout = os.path.join(td, "out.bin")
+        write_input(fin, p)
+        res = subprocess.run([BINARY, fin, fout, "pertrb"], capture_output=True, text=True, timeout=timeout)
+        if res.returncode != 0:
+            raise RuntimeError(f"hw3crt_run failed: {res.stderr}")
+        pertrb = ierror = None
+        for line in res.stdout.splitlines():
+            if line.startswith("pertrb"):
+                parts = line.split()
+                pertrb, ierror = float(parts[1]), int(parts[3])
+        u = np.fromfile(fout, dtype="<f8").reshape(p["nz"] + 1, p["ny"] + 1, p["nx"] + 1)
+    return u, pertrb, ierror
+
+
 def solve_many_parallel(p, procs, timeout=3600):
     """Runs ``procs`` independent copies of the same solve concurrently (one
     process each; hw3crt is serial).  Returns the per-process wall times."""

@@ -18,6 +18,13 @@
 //   stdout     : "hw3crt_seconds <best> <median> <repeats>"
 //
 // usage: hw3crt_run <in.bin> <out.bin> [repeats]
+//        hw3crt_run <in.bin> <out.bin> pertrb
+//   The second form calls hw3crt_ (declared by the reference's
+//   hw3crt_wrapper.h) directly, once, with the wrapper's arguments and a
+//   workspace twice the wrapper's size, and also prints
+//   "pertrb <value> ierror <code>": the wrapper computes PERTRB (the constant
+//   FISHPACK subtracts from F when lambda = 0 and no boundary pins the
+//   solution) but does not return it.
 #include <chrono>
 #include <cstdint>
 #include <cstdio>
@@ -37,7 +44,8 @@ int main(int argc, char** argv) {
         fprintf(stderr, "usage: %s in.bin out.bin [repeats]\n", argv[0]);
         return 2;
     }
-    int repeats = argc > 3 ? atoi(argv[3]) : 1;
+    const bool want_pertrb = argc > 3 && std::strcmp(argv[3], "pertrb") == 0;
+    int repeats = (argc > 3 && !want_pertrb) ? atoi(argv[3]) : 1;
     if (repeats < 1) repeats = 1;
 
     FILE* fp = fopen(argv[1], "rb");
@@ -76,6 +84,24 @@ int main(int argc, char** argv) {
     fclose(fp);
 
     std::vector<double> f(npts);
+    if (want_pertrb) {
+        std::memcpy(f.data(), f0.data(), npts * sizeof(double));
+        int l = nx, m = ny, n = nz, lb = xbc, mb = ybc, nb = zbc, ldimf = nx + 1, mdimf = ny + 1;
+        double xs = dom[0], xf = dom[1], ys = dom[2], yf = dom[3], zs = dom[4], zf = dom[5], lam = dom[6];
+        const int wsize = 2 * (30 + l + m + 5 * n + std::max(std::max(l, m), n) + 7 * ((l + 1) / 2 + (m + 1) / 2));
+        std::vector<double> w(wsize);
+        double pertrb = 0.0;
+        int ierror = -1;
+        hw3crt_(&xs, &xf, &l, &lb, fp_face[0], fp_face[1], &ys, &yf, &m, &mb, fp_face[2], fp_face[3],
+                &zs, &zf, &n, &nb, fp_face[4], fp_face[5], &lam, &ldimf, &mdimf, f.data(), &pertrb, &ierror,
+                w.data());
+        printf("pertrb %.17g ierror %d\n", pertrb, ierror);
+        FILE* fo = fopen(argv[2], "wb");
+        if (!fo) { perror("open output"); return 2; }
+        if (fwrite(f.data(), sizeof(double), npts, fo) != npts) { fprintf(stderr, "short write\n"); return 2; }
+        fclose(fo);
+        return 0;
+    }
     std::vector<double> times;
     for (int r = 0; r < repeats; ++r) {
         std::memcpy(f.data(), f0.data(), npts * sizeof(double));

@@ -111,3 +111,32 @@ def residual(u, f, nx, ny, nz, xbc, ybc, zbc, dom, lam, faces):
     r[w] = np.asarray(f)[w] - apply_operator(uu, nx, ny, nz, xbc, ybc, zbc,
                                              dom, lam, faces)[w]
     return r
+
+
+def singular_pertrb(p):
+    """FISHPACK's PERTRB for the singular case (lambda = 0, every code 0 or 3):
+    the constant hw3crt subtracts from the right-hand side so that a solution
+    exists (the wrapper passes &pertrb to hw3crt_ and drops it,
+    cudahelmholtz/hw3crt_wrapper.cpp:20-28).  On this discrete system it is
+    the weighted mean of b = f + boundary terms over the unknown window, with
+    weight 1/2 per Neumann boundary index (the weights under which the operator
+    is symmetric); 0 when the problem is not singular.  Pinned against the
+    runner's direct hw3crt call (tests/golden/fishpack_singular.npz)."""
+    nx, ny, nz = p["nx"], p["ny"], p["nz"]
+    bcs = (p["xbc"], p["ybc"], p["zbc"])
+    if p["lam"] != 0.0 or any(b not in (0, 3) for b in bcs):
+        return 0.0
+    faces = {k: p.get(k) for k in FACE_KEYS}
+    zero = np.zeros((nz + 1, ny + 1, nx + 1))
+    # A_h of the zero field with the Neumann data is minus the boundary terms
+    terms = -apply_operator(zero, nx, ny, nz, *bcs, p["dom"], 0.0, faces)
+    w = window_slices(nx, ny, nz, *bcs)
+    b = (np.asarray(p["f"], dtype=np.float64) + terms)[w]
+    wt = np.ones_like(b)
+    for axis, bc in ((0, p["zbc"]), (1, p["ybc"]), (2, p["xbc"])):
+        if bc == 3:
+            for end in (0, -1):
+                sl = [slice(None)] * 3
+                sl[axis] = end
+                wt[tuple(sl)] *= 0.5
+    return float((wt * b).sum() / wt.sum())

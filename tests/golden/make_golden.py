@@ -10,6 +10,9 @@ reference's CPU path run in this repository's build container:
 * fishpack_sweep_10x6x8.npz  -- all 125 boundary-code triples on a 10x6x8 grid,
   lambda = -3.7, f and Neumann data ~ U[-1, 1] (periodic-compatible);
 * fishpack_16x12x20.npz      -- 12 triples on 16x12x20 with varied lambda;
+* fishpack_singular.npz      -- lambda = 0 with every code 0 or 3 on 16x12x20
+  and 10x14x8: the solution and PERTRB of a direct hw3crt call (the runner's
+  "pertrb" mode; the wrapper drops PERTRB);
 * fishpack_ufunc_case1.npz   -- the reference's analytic case 1 (ufunc.h:12-32,
   u = sin(2 pi x) sin(2 pi y) sin(2 pi z) / 3, lambda = -1) on 32^3 and
   24x20x28 for a few triples, with fishpack's max-norm error.
@@ -111,6 +114,11 @@ def ufunc_problem(nx, ny, nz, xbc, ybc, zbc):
     return p
 
 
+SINGULAR_CASES = [  # (dims, codes, seed), lambda = 0
+    ((16, 12, 20), (3, 3, 3), 3000), ((16, 12, 20), (0, 3, 0), 3001), ((16, 12, 20), (0, 0, 0), 3002),
+    ((16, 12, 20), (3, 0, 3), 3003), ((10, 14, 8), (0, 0, 3), 3004), ((10, 14, 8), (3, 3, 0), 3005),
+]
+
 UFUNC_CASES = [((32, 32, 32), (1, 2, 0)), ((32, 32, 32), (3, 4, 0)),
                ((24, 20, 28), (1, 2, 3)), ((24, 20, 28), (4, 3, 1))]
 
@@ -144,6 +152,22 @@ def main():
                         dims=np.array(MID_DIMS), cases=np.array(MID_CASES),
                         seeds=np.array(seeds), digests=np.array(digests),
                         u=np.stack(us))
+    # singular problems: solution and PERTRB of a direct hw3crt call
+    us, pert, digests = [], [], []
+    for dims, bcs, seed in SINGULAR_CASES:
+        p = gen.random_problem(*dims, *bcs, 0.0, seed)
+        u, pertrb, ierror = fishpack.solve_with_pertrb(p)
+        if ierror != 0:
+            raise SystemExit(f"hw3crt ierror {ierror} on {dims} {bcs}")
+        us.append(u.ravel())
+        pert.append(pertrb)
+        digests.append(input_digest(p))
+    np.savez_compressed(os.path.join(HERE, "fishpack_singular.npz"),
+                        dims=np.array([c[0] for c in SINGULAR_CASES]),
+                        codes=np.array([c[1] for c in SINGULAR_CASES]),
+                        seeds=np.array([c[2] for c in SINGULAR_CASES]), digests=np.array(digests),
+                        u=np.concatenate(us), offsets=np.cumsum([0] + [len(v) for v in us]),
+                        pertrb=np.array(pert))
     # analytic case 1
     rec = []
     for dims, bcs in UFUNC_CASES:

@@ -141,3 +141,37 @@ def test_residual_of_emulated_solution_is_small():
 def test_oracle_rejects_bad_boundary_code():
     with pytest.raises(ValueError):
         E.solver_windows(5, 8)
+
+
+def _singular_cases():
+    g = _load_golden("fishpack_singular.npz")
+    out = []
+    for t in range(len(g["pertrb"])):
+        dims = tuple(int(v) for v in g["dims"][t])
+        codes = tuple(int(v) for v in g["codes"][t])
+        p = gen.random_problem(*dims, *codes, 0.0, int(g["seeds"][t]))
+        u = g["u"][g["offsets"][t]:g["offsets"][t + 1]].reshape(dims[2] + 1, dims[1] + 1, dims[0] + 1)
+        out.append((p, u, float(g["pertrb"][t]), str(g["digests"][t])))
+    return out
+
+
+def test_singular_pertrb_matches_fishpack():
+    """lambda = 0, every code 0 or 3: the oracle's PERTRB (weighted mean of the
+    right-hand side) equals hw3crt's, and the reference GPU path's zero-mode
+    solution differs from hw3crt's unnormalised one by a constant only."""
+    import sys
+    sys.path.insert(0, GOLDEN)
+    from make_golden import input_digest  # noqa: E402
+    for p, u_ref, pert_ref, digest in _singular_cases():
+        assert input_digest(p) == digest
+        pert = stencil.singular_pertrb(p)
+        assert abs(pert - pert_ref) <= 1e-12 * max(1.0, abs(pert_ref)), (pert, pert_ref)
+        d = _solve_emulated(p) - u_ref
+        assert np.ptp(d) <= 1e-12 * np.linalg.norm(u_ref), np.ptp(d)
+
+
+def test_pertrb_is_zero_when_not_singular():
+    p = gen.random_problem(16, 12, 20, 1, 3, 3, 0.0, seed=1)
+    assert stencil.singular_pertrb(p) == 0.0
+    p = gen.random_problem(16, 12, 20, 3, 3, 3, -1.0, seed=1)
+    assert stencil.singular_pertrb(p) == 0.0
