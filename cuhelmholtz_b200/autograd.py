@@ -93,3 +93,129 @@ def helmholtz_solve(f: torch.Tensor, lam, dims: Sequence[int], bcs: Sequence[int
     spec = _Spec(dims, bcs, dom, precision, corrections)
     ft = [faces.get(k) for k in FACE_KEYS]
     return HelmholtzSolveFunction.apply(f, lam, *ft, spec)
+
+
+# ---------------------------------------------------------------------------
+# do_transform as a differentiable function
+# ---------------------------------------------------------------------------
+#
+# Each kind is a matrix from its input window to its output window
+# (funcinterface.cu:25-40 and the per-kind files cudasymmfft/dst1..dct3,
+# dftfunc.cu; the formulas with the reference's "half FFTW" scaling); its
+# transpose is another kind between two diagonal scalings along the line:
+#   DST_1^T = DST_1                     DCT_1^T = W DCT_1 W^-1 (W = 1/2 at 0, N)
+#   DST_2^T g = DST_3(g; g[0] = 0, g[N] doubled)
+#   DST_3^T g = DST_2(g) with entry N halved and copied to entry 0 (DST_3 also
+#               reads x[0] through its 1/2 (x[0] + x[N]) term)
+#   DCT_2^T g = DCT_3(g with g[0] doubled)      DCT_3^T g = DCT_2(g), entry 0 halved
+#   R2C^T g = C2R(g with the interior bins halved)
+#   C2R^T g = R2C(g) with the interior bins doubled
+# The 3-D transform is the tensor product of the three axes' matrices, so its
+# transpose applies the three transposes (each axis' scalings commute with the
+# other axes' transforms).
+
+from .api import (DCT_1, DCT_2, DCT_3, DST_1, DST_2, DST_3, DFT_C2R, DFT_R2C,  # noqa: E402
+                  do_transform, padded_numel)
+
+_ADJOINT_KIND = {DST_1: DST_1, DST_2: DST_3, DST_3: DST_2, DCT_1: DCT_1, DCT_2: DCT_3, DCT_3: DCT_2,
+                 DFT_R2C: DFT_C2R, DFT_C2R: DFT_R2C}
+
+
+# input and output windows [lo, hi] of each kind on a padded line of N + 2
+# entries (the per-kind pre/post kernels' loads and stores, dst1..dct3 and
+# dftfunc.cu; an out-of-place transform leaves intermediate values elsewhere)
+_IN_WIN = {DST_1: lambda n: (1, n - 1), DST_2: lambda n: (1, n), DST_3: lambda n: (0, n),
+           DCT_1: lambda n: (0, n), DCT_2: lambda n: (0, n - 1), DCT_3: lambda n: (0, n - 1),
+           DFT_R2C: lambda n: (0, n - 1), DFT_C2R: lambda n: (0, n + 1)}
+_OUT_WIN = {DST_1: lambda n: (0, n - 1), DST_2: lambda n: (0, n), DST_3: lambda n: (0, n),
+            DCT_1: lambda n: (0, n), DCT_2: lambda n: (0, n - 1), DCT_3: lambda n: (0, n - 1),
+            DFT_R2C: lambda n: (0, n + 1), DFT_C2R: lambda n: (0, n - 1)}
+
+
+def _mask(win, n, device):
+    lo, hi = win(n)
+    m = torch.zeros(n + 2, dtype=torch.float64, device=device)
+    m[lo:hi + 1] = 1.0
+    return m
+
+
+def _pre_weights(kind, n, device):
+    """Scaling of the output gradient (length n + 2) before the adjoint kind."""
+    w = torch.ones(n + 2, dtype=torch.float64, device=device)
+    if kind == DST_2:
+        w[0] = 0.0
+        w[n] = 2.0
+    elif kind == DCT_1:
+        w[0] = 2.0
+        w[n] = 2.0
+    elif kind == DCT_2:
+        w[0] = 2.0
+    elif kind == DFT_R2C:
+        w[2:n] = 0.5
+    return w
+
+
+def _post_weights(kind, n, device):
+    """Scaling of the adjoint kind's output (length n + 2)."""
+    w = torch.ones(n + 2, dtype=torch.float64, device=device)
+    if kind == DST_3:
+        w[n] = 0.5
+    elif kind == DCT_1:
+        w[0] = 0.5
+        w[n] = 0.5
+    elif kind == DCT_3:
+        w[0] = 0.5
+    elif kind == DFT_C2R:
+        w[2:n] = 2.0
+        w[1] = 0.0
+        w[n + 1] = 0.0
+    return w
+
+
+def _scale3(t, wx, wy, wz):
+    return t * wz.view(-1, 1, 1) * wy.view(1, -1, 1) * wx.view(1, 1, -1)
+
+
+class TransformFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, nx, ny, nz, kx, ky, kz):
+        src = x.detach().contiguous().view(-1)
+        out = torch.zeros(padded_numel(nx, ny, nz), dtype=torch.float64, device=x.device)
+        do_transform(src, out, nx, ny, nz, kx, ky, kz)
+        dev = x.device
+        out = _scale3(out.view(nz + 2, ny + 2, nx + 2), _mask(_OUT_WIN[kx], nx, dev),
+                      _mask(_OUT_WIN[ky], ny, dev), _mask(_OUT_WIN[kz], nz, dev))
+        ctx.dims = (nx, ny, nz)
+        ctx.kinds = (kx, ky, kz)
+        return out.reshape(x.shape)
+
+    @staticmethod
+    def backward(ctx, g):
+        nx, ny, nz = ctx.dims
+        kx, ky, kz = ctx.kinds
+        dev = g.device
+        g3 = g.contiguous().view(nz + 2, ny + 2, nx + 2).to(torch.float64)
+        gin = _scale3(g3, _pre_weights(kx, nx, dev), _pre_weights(ky, ny, dev), _pre_weights(kz, nz, dev))
+        gin = gin.contiguous().view(-1)
+        res = torch.zeros_like(gin)
+        do_transform(gin, res, nx, ny, nz, _ADJOINT_KIND[kx], _ADJOINT_KIND[ky], _ADJOINT_KIND[kz])
+        res = _scale3(res.view(nz + 2, ny + 2, nx + 2), _post_weights(kx, nx, dev) * _mask(_IN_WIN[kx], nx, dev),
+                      _post_weights(ky, ny, dev) * _mask(_IN_WIN[ky], ny, dev),
+                      _post_weights(kz, nz, dev) * _mask(_IN_WIN[kz], nz, dev))
+        # DST_3 reads x[0] with the weight of x[N]
+        if kx == DST_3:
+            res[:, :, 0] = res[:, :, nx]
+        if ky == DST_3:
+            res[:, 0, :] = res[:, ny, :]
+        if kz == DST_3:
+            res[0, :, :] = res[nz, :, :]
+        return res.reshape(g.shape), None, None, None, None, None, None
+
+
+def transform(x: torch.Tensor, nx: int, ny: int, nz: int, kx: int, ky: int, kz: int) -> torch.Tensor:
+    """Differentiable 3-D mixed transform (the reference's do_transform kinds)
+    of the padded (NZ+2, NY+2, NX+2) float64 CUDA tensor ``x`` (any shape with
+    that many elements), out of place: entries outside the kinds' output
+    windows are 0 (where do_transform leaves them undefined), entries outside
+    their input windows do not contribute (their gradient is 0)."""
+    return TransformFunction.apply(x, nx, ny, nz, int(kx), int(ky), int(kz))
