@@ -7,7 +7,7 @@ mirror of the reference's interface over that ABI.  There is no CPU fallback.
 """
 from .api import (  # noqa: F401
     BatchPlan, CHZError, DCT_1, DCT_2, DCT_3, DST_1, DST_2, DST_3, DFT_R2C, DFT_C2R, KIND_NAMES,
-    cuda_helmholtz_solver, do_transform, helmholtz_solve_pertrb, helmholtz_solve_refined, padded_numel, set_kernel_family,
+    cuda_helmholtz_solver, do_transform, helmholtz_solve_19pt, helmholtz_solve_pertrb, helmholtz_solve_refined, padded_numel, set_kernel_family,
     solve_problem, workspace_size,
 )
 from ._lib import lib, library_path  # noqa: F401

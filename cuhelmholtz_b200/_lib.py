@@ -33,6 +33,9 @@ SIGNATURES = {
                                     c_double, c_double, c_int, c_int, _dp, _dp,
                                     c_double, c_double, c_int, c_int, _dp, _dp,
                                     c_double, _dp, c_void_p]),
+    "chz_helmholtz_solve_19pt": (c_int, [c_double, c_double, c_int, c_int, _dp, _dp, c_double, c_double, c_int,
+                                         c_int, _dp, _dp, c_double, c_double, c_int, c_int, _dp, _dp, c_double,
+                                         _dp, c_void_p]),
     "chz_helmholtz_solve_pertrb": (c_int, [c_double, c_double, c_int, c_int, _dp, _dp, c_double, c_double, c_int,
                                            c_int, _dp, _dp, c_double, c_double, c_int, c_int, _dp, _dp, c_double,
                                            _dp, ctypes.POINTER(c_double), c_void_p]),

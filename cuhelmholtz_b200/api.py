@@ -120,6 +120,26 @@ def cuda_helmholtz_solver(left, right, NX, xbc, bcl, bcr,
     return 0
 
 
+def helmholtz_solve_19pt(left, right, NX, xbc, bcl, bcr,
+                         bottom, top, NY, ybc, bcb, bct,
+                         front, back, NZ, zbc, bcf, bce,
+                         lambda_, f, stream=None) -> int:
+    """cuda_helmholtz_solver with the reference's 19-point division (compact
+    fourth-order Laplacian, filtered right-hand side): codes 1 and 3 and one
+    grid spacing on all axes.  In place on ``f``."""
+    n = (NX + 1) * (NY + 1) * (NZ + 1)
+    pf = _ptr(f, "f", n)
+    fx, fy, fz = (_face_len(a, NX, NY, NZ) for a in "xyz")
+    faces = [_ptr(bcl, "bcl", fx), _ptr(bcr, "bcr", fx), _ptr(bcb, "bcb", fy),
+             _ptr(bct, "bct", fy), _ptr(bcf, "bcf", fz), _ptr(bce, "bce", fz)]
+    _check(_lib.lib().chz_helmholtz_solve_19pt(
+        float(left), float(right), NX, xbc, faces[0], faces[1],
+        float(bottom), float(top), NY, ybc, faces[2], faces[3],
+        float(front), float(back), NZ, zbc, faces[4], faces[5],
+        float(lambda_), pf, _stream(stream)))
+    return 0
+
+
 def helmholtz_solve_pertrb(left, right, NX, xbc, bcl, bcr,
                            bottom, top, NY, ybc, bcb, bct,
                            front, back, NZ, zbc, bcf, bce,

@@ -248,13 +248,37 @@ int check_faces(const AxisSolve& a, const double* lo, const double* hi, const ch
     return CHZ_SUCCESS;
 }
 
+// Division of the 19-point variant (_nonpoisson_devide_19points_,
+// _cuda_helmholtz_.inl:255-274, left commented out in the reference at
+// cuda_helmholtz_solver.cu:325,338): on the spectral window, with
+// c_a = cos(m_a pi / N_a),
+//   value *= (1/2 + (c_i + c_j + c_k) / 6)
+//          / ((2/3 (c_i c_j + c_i c_k + c_j c_k + c_i + c_j + c_k) - 4) h^-2 + lambda)
+// -- the eigenvalues of the compact 19-point Laplacian and of its 7-point
+// right-hand-side filter.  The mode (0,0,0) is set to 0 when its denominator
+// is 0 (lambda = 0, Neumann on every axis), where the reference divides by 0.
+__global__ void divide19(double* ws, long long wy, long long wz, int xs, int xe, int ys, int ys_n, int zs,
+                         double pix, double piy, double piz, double d2, double lam, int zero_mode) {
+    const int i = xs + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = ys + blockIdx.y;
+    const int k = zs + blockIdx.z;
+    if (i > xe || j >= ys + ys_n) return;
+    const double ci = cos(i * pix), cj = cos(j * piy), ck = cos(k * piz);
+    const double coef = (2.0 / 3.0 * (ci * cj + ci * ck + cj * ck + ci + cj + ck) - 4.0) * d2 + lam;
+    const double filt = 0.5 + (ci + cj + ck) / 6.0;
+    const long long o = k * wz + j * wy + i;
+    ws[o] = (zero_mode && i == 0 && j == 0 && k == 0) ? 0.0 : ws[o] * filt / coef;
+}
+
 // The five line passes and the periodic planes of one FP64 solve, with the
-// per-axis tables and the work array given by the caller.
+// per-axis tables and the work array given by the caller.  stencil19: the
+// z pass is split around the 19-point division (divide19) instead of fusing
+// the 7-point one.
 int run_solve_passes(const AxisSolve& X, const AxisSolve& Y, const AxisSolve& Z, const DeviceLineTables& tx,
                      const DeviceLineTables& ty, const DeviceLineTables& tz, const double* ex, const double* ey,
                      const double* ez, const double* bcl, const double* bcr, const double* bcb,
                      const double* bct, const double* bcf, const double* bce, double lambda, double* f,
-                     double* ws, cudaStream_t s) {
+                     double* ws, cudaStream_t s, bool stencil19) {
     int rc;
     const int nx = X.n, ny = Y.n, nz = Z.n;
     const long long fy = nx + 1, fz = (long long)(nx + 1) * (ny + 1);
@@ -301,7 +325,34 @@ int run_solve_passes(const AxisSolve& X, const AxisSolve& Y, const AxisSolve& Z,
         if (rc) return cuda_fail(rc, "solver pass 2");
     }
     // pass 3: z forward, eigenvalue division, z inverse, in place
-    {
+    if (stencil19) {
+        const LineGeom g = line_geometry(nz, 1, false);
+        PassArgs a{};
+        a.kind = Z.kf; a.kind2 = -1;
+        a.u0 = X.sp0; a.nu = X.sp1 - X.sp0 + 1; a.v0 = Y.sp0;
+        a.in_su = 1; a.in_sv = wy; a.in_sl = wz;
+        a.ld_lo = Z.s; a.ld_hi = Z.e;
+        a.out_su = 1; a.out_sv = wy; a.out_sl = wz;
+        a.st_lo = Z.sp0; a.st_hi = Z.sp1;
+        a.scale = 1.0; a.use_scale = 0;
+        a.PR = g.PR; a.log2W = g.log2W;
+        rc = launch_line_pass(1, kIoF64, kIoF64, false, ws, ws, a, tz, g, Y.sp1 - Y.sp0 + 1, s, "solve19_z_fwd");
+        if (rc) return cuda_fail(rc, "solver pass 3 (forward)");
+        const dim3 blk(128, 1, 1);
+        const dim3 grd((X.sp1 - X.sp0 + 128) / 128, Y.sp1 - Y.sp0 + 1, Z.sp1 - Z.sp0 + 1);
+        const bool zm = lambda == 0.0 && X.bc == 3 && Y.bc == 3 && Z.bc == 3;
+        trace_begin(s, "solve19_divide");
+        divide19<<<grd, blk, 0, s>>>(ws, wy, wz, X.sp0, X.sp1, Y.sp0, Y.sp1 - Y.sp0 + 1, Z.sp0, X.pidiv, Y.pidiv,
+                                      Z.pidiv, X.d2, lambda, zm ? 1 : 0);
+        count_launch();
+        trace_end(s);
+        if ((rc = (int)cudaGetLastError())) return cuda_fail(rc, "19-point division");
+        a.kind = Z.ki;
+        a.ld_lo = Z.sp0; a.ld_hi = Z.sp1;
+        a.st_lo = Z.s; a.st_hi = Z.e;
+        rc = launch_line_pass(1, kIoF64, kIoF64, false, ws, ws, a, tz, g, Y.sp1 - Y.sp0 + 1, s, "solve19_z_inv");
+        if (rc) return cuda_fail(rc, "solver pass 3 (inverse)");
+    } else {
         const LineGeom g = line_geometry(nz, 1, false);
         PassArgs a{};
         a.kind = Z.kf; a.kind2 = Z.ki;
@@ -363,14 +414,15 @@ namespace {
 
 int solve_fp64(const AxisSolve& X, const AxisSolve& Y, const AxisSolve& Z, const double* bcl,
                const double* bcr, const double* bcb, const double* bct, const double* bcf,
-               const double* bce, double lambda, double* f, double* ws, cudaStream_t s) {
+               const double* bce, double lambda, double* f, double* ws, cudaStream_t s, bool stencil19 = false) {
     int rc;
     DeviceLineTables tx, ty, tz;
     if ((rc = tables_for(X.n, 1, &tx)) || (rc = tables_for(Y.n, 1, &ty)) || (rc = tables_for(Z.n, 1, &tz)))
         return rc;
     const double *ex, *ey, *ez;
     if ((rc = eig_table(X, &ex)) || (rc = eig_table(Y, &ey)) || (rc = eig_table(Z, &ez))) return rc;
-    return run_solve_passes(X, Y, Z, tx, ty, tz, ex, ey, ez, bcl, bcr, bcb, bct, bcf, bce, lambda, f, ws, s);
+    return run_solve_passes(X, Y, Z, tx, ty, tz, ex, ey, ez, bcl, bcr, bcb, bct, bcf, bce, lambda, f, ws, s,
+                            stencil19);
 }
 
 // Library-owned workspaces, one grow-only buffer per (device, stream).
@@ -412,13 +464,24 @@ namespace {
 int solve_common(double left, double right, int nx, int xbc, const double* bcl, const double* bcr,
                  double bottom, double top, int ny, int ybc, const double* bcb, const double* bct,
                  double front, double back, int nz, int zbc, const double* bcf, const double* bce,
-                 double lambda, double* f, void* ws, size_t ws_bytes, bool own_ws, void* stream) {
+                 double lambda, double* f, void* ws, size_t ws_bytes, bool own_ws, void* stream,
+                 bool stencil19 = false) {
     g_last_error[0] = 0;
     int rc;
     AxisSolve X, Y, Z;
     if ((rc = setup_axis(nx, xbc, left, right, &X)) || (rc = setup_axis(ny, ybc, bottom, top, &Y)) ||
         (rc = setup_axis(nz, zbc, front, back, &Z)))
         return rc;
+    if (stencil19) {
+        // the reference's 19-point division takes one grid spacing (dx2) and
+        // no half-sample shift: cubic cells, codes 1 and 3
+        auto ok = [](int bc) { return bc == 1 || bc == 3; };
+        if (!ok(X.bc) || !ok(Y.bc) || !ok(Z.bc))
+            return fail(CHZ_ERROR_INVALID_VALUE, "the 19-point solve takes boundary codes 1 and 3 only");
+        const double tol = 1e-12 * X.d2;
+        if (std::fabs(X.d2 - Y.d2) > tol || std::fabs(X.d2 - Z.d2) > tol)
+            return fail(CHZ_ERROR_INVALID_VALUE, "the 19-point solve needs equal grid spacing on all axes");
+    }
     if ((rc = check_len(nx, "x")) || (rc = check_len(ny, "y")) || (rc = check_len(nz, "z"))) return rc;
     if (!f) return fail(CHZ_ERROR_INVALID_VALUE, "f is NULL");
     if ((rc = check_faces(X, bcl, bcr, "x")) || (rc = check_faces(Y, bcb, bct, "y")) ||
@@ -432,7 +495,7 @@ int solve_common(double left, double right, int nx, int xbc, const double* bcl, 
             return fail(CHZ_ERROR_WORKSPACE, "workspace needs %zu bytes, 256-byte aligned", need);
     }
     return solve_fp64(X, Y, Z, bcl, bcr, bcb, bct, bcf, bce, lambda, f, static_cast<double*>(ws),
-                      static_cast<cudaStream_t>(stream));
+                      static_cast<cudaStream_t>(stream), stencil19);
 }
 
 }  // namespace
@@ -482,6 +545,14 @@ size_t chz_helmholtz_workspace_size(int nx, int ny, int nz, int precision) {
         bytes = r256(pe32 * sizeof(float)) + r256((size_t)(nx + 1) * (ny + 1) * (nz + 1) * sizeof(double)) + 256;
     }
     return (bytes + 255) & ~(size_t)255;
+}
+
+int chz_helmholtz_solve_19pt(double left, double right, int nx, int xbc, const double* bcl, const double* bcr,
+                             double bottom, double top, int ny, int ybc, const double* bcb, const double* bct,
+                             double front, double back, int nz, int zbc, const double* bcf, const double* bce,
+                             double lambda, double* f, void* stream) {
+    return solve_common(left, right, nx, xbc, bcl, bcr, bottom, top, ny, ybc, bcb, bct, front, back, nz, zbc, bcf,
+                        bce, lambda, f, nullptr, 0, true, stream, true);
 }
 
 int chz_helmholtz_solve(double left, double right, int nx, int xbc, const double* bcl, const double* bcr,

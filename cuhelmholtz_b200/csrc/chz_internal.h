@@ -151,7 +151,7 @@ int run_solve_passes(const AxisSolve& X, const AxisSolve& Y, const AxisSolve& Z,
                      const DeviceLineTables& ty, const DeviceLineTables& tz, const double* ex, const double* ey,
                      const double* ez, const double* bcl, const double* bcr, const double* bcb,
                      const double* bct, const double* bcf, const double* bce, double lambda, double* f,
-                     double* ws, cudaStream_t s);
+                     double* ws, cudaStream_t s, bool stencil19 = false);
 extern thread_local char g_last_error[512];
 int current_device();
 int tables_for(int n, int is_double, DeviceLineTables* t);

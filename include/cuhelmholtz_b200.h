@@ -84,6 +84,23 @@ int chz_helmholtz_solve(double left, double right, int nx, int xbc,
 
 /* As chz_helmholtz_solve with a caller-owned device workspace of at least
  * chz_helmholtz_workspace_size(nx, ny, nz, 0) bytes, 256-byte aligned. */
+/* The solve with the reference's 19-point variant (_nonpoisson_devide_19points_,
+ * _cuda_helmholtz_.inl:255-274, commented out at cuda_helmholtz_solver.cu:325
+ * and :338): the spectral division by the eigenvalues of the compact 19-point
+ * Laplacian, (2/3 (ci cj + ci ck + cj ck + ci + cj + ck) - 4) / h^2 + lambda,
+ * with the right-hand side filtered by 1/2 + (ci + cj + ck) / 6,
+ * ca = cos(m pi / N); the boundary terms are the 7-point solve's.  As the
+ * reference kernel: one grid spacing on all axes and codes 1 and 3 only
+ * (CHZ_ERROR_INVALID_VALUE otherwise).  Mode (0,0,0) of an all-Neumann
+ * lambda = 0 problem is set to 0 (the reference divides by 0 there). */
+int chz_helmholtz_solve_19pt(double left, double right, int nx, int xbc,
+                             const double* bcl, const double* bcr,
+                             double bottom, double top, int ny, int ybc,
+                             const double* bcb, const double* bct,
+                             double front, double back, int nz, int zbc,
+                             const double* bcf, const double* bce,
+                             double lambda, double* f, void* stream);
+
 /* Helmholtz solve as chz_helmholtz_solve that also returns PERTRB, as
  * FISHPACK's hw3crt does (hw3crt_wrapper.cpp:20-28 passes &pertrb to hw3crt_
  * but does not return it): when lambda = 0 and every code is 0 or 3 the

@@ -359,10 +359,14 @@ def _c_int_ratio(nx: int, ny: int, nz: int) -> int:
 def emulate_solver(left, right, nx, xbc, bcl, bcr,
                    bottom, top, ny, ybc, bcb, bct,
                    front, back, nz, zbc, bcf, bce,
-                   lam, f):
+                   lam, f, stencil19=False):
     """Returns the array the reference writes into ``f`` (shape (NZ+1, NY+1,
     NX+1), [z][y][x]).  Face arrays: x faces (NZ+1, NY+1), y faces
     (NZ+1, NX+1), z faces (NY+1, NX+1), as laid out in testgpurectangle.cu:46-57.
+
+    stencil19: the non-periodic branch divides with the reference's
+    _nonpoisson_devide_19points_ (_cuda_helmholtz_.inl:255-274; its call is
+    commented out at cuda_helmholtz_solver.cu:338) instead of _divide_.
     """
     f = np.array(f, dtype=np.float64, copy=True).reshape(nz + 1, ny + 1, nx + 1)
     dx = nx / (right - left)
@@ -450,6 +454,17 @@ def emulate_solver(left, right, nx, xbc, bcl, bcr,
     den = ((ex_[None, None, :] + ey_[None, :, None]) + ez_[:, None, None]) + lam
     with np.errstate(divide="ignore"):
         eig = 1.0 / den
+    if stencil19:
+        # cos(i * pidivnx) etc. (no shift), dx2 only, no zero-mode handling
+        if 0 in (xbc, ybc, zbc):
+            raise ValueError("the 19-point division is the non-periodic branch's")
+        ci = np.cos(mi * pidiv["x"])[None, None, :]
+        cj = np.cos(mj * pidiv["y"])[None, :, None]
+        ck = np.cos(mk * pidiv["z"])[:, None, None]
+        coef = (2.0 / 3.0 * (ci * cj + ci * ck + cj * ck + ci + cj + ck) - 4) * dx2 + lam
+        with np.errstate(divide="ignore", invalid="ignore"):
+            eig = (0.5 + 1.0 / 6.0 * (ci + cj + ck)) / coef
+        needperturb = False
     if needperturb and mi[0] == 0 and mj[0] == 0 and mk[0] == 0:
         eig[0, 0, 0] = 0.0
     for ek in ent_k:

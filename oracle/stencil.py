@@ -140,3 +140,50 @@ def singular_pertrb(p):
                 sl[axis] = end
                 wt[tuple(sl)] *= 0.5
     return float((wt * b).sum() / wt.sum())
+
+
+def _extend(u, codes):
+    """u on the unknown window, extended by one ghost layer per axis with the
+    homogeneous closures of codes 1 (Dirichlet neighbour 0) and 3 (mirror)."""
+    e = np.asarray(u, dtype=np.float64)
+    for axis, bc in ((0, codes[2]), (1, codes[1]), (2, codes[0])):
+        e = np.moveaxis(e, axis, -1)
+        if bc == 1:
+            lo = np.zeros_like(e[..., :1])
+            hi = np.zeros_like(e[..., :1])
+        elif bc == 3:
+            lo = e[..., 1:2]
+            hi = e[..., -2:-1]
+        else:
+            raise ValueError("codes 1 and 3 only")
+        e = np.concatenate([lo, e, hi], axis=-1)
+        e = np.moveaxis(e, -1, axis)
+    return e
+
+
+def apply_19pt(u, codes, h2):
+    """The compact 19-point Laplacian (1 / (6 h^2)) (-24 u + 2 sum of the 6 face
+    neighbours + sum of the 12 edge neighbours) on the unknown window, with
+    homogeneous closures (codes 1 and 3)."""
+    e = _extend(u, codes)
+    c = e[1:-1, 1:-1, 1:-1]
+    faces = (e[:-2, 1:-1, 1:-1] + e[2:, 1:-1, 1:-1] + e[1:-1, :-2, 1:-1] + e[1:-1, 2:, 1:-1]
+             + e[1:-1, 1:-1, :-2] + e[1:-1, 1:-1, 2:])
+    edges = 0.0
+    sl = {-1: slice(0, -2), 0: slice(1, -1), 1: slice(2, None)}
+    for dz in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                if abs(dz) + abs(dy) + abs(dx) == 2:
+                    edges = edges + e[sl[dz], sl[dy], sl[dx]]
+    return (-24.0 * c + 2.0 * faces + edges) * h2 / 6.0
+
+
+def filter_19pt(b, codes):
+    """Right-hand-side filter of the compact scheme, (6 b + sum of the 6 face
+    neighbours) / 12, with the same closures."""
+    e = _extend(b, codes)
+    c = e[1:-1, 1:-1, 1:-1]
+    faces = (e[:-2, 1:-1, 1:-1] + e[2:, 1:-1, 1:-1] + e[1:-1, :-2, 1:-1] + e[1:-1, 2:, 1:-1]
+             + e[1:-1, 1:-1, :-2] + e[1:-1, 1:-1, 2:])
+    return (6.0 * c + faces) / 12.0

@@ -175,3 +175,42 @@ def test_pertrb_is_zero_when_not_singular():
     assert stencil.singular_pertrb(p) == 0.0
     p = gen.random_problem(16, 12, 20, 3, 3, 3, -1.0, seed=1)
     assert stencil.singular_pertrb(p) == 0.0
+
+
+def _rhs_with_terms(p):
+    """b = f + boundary terms on the unknown window (the 7-point solve's)."""
+    n = (p["nx"], p["ny"], p["nz"])
+    codes = (p["xbc"], p["ybc"], p["zbc"])
+    d = p["dom"]
+    w = stencil.window_slices(*n, *codes)
+    f = np.asarray(p["f"], dtype=np.float64)
+    neumann = -stencil.apply_operator(np.zeros_like(f), *n, *codes, d, 0.0,
+                                      {k: p.get(k) for k in stencil.FACE_KEYS})
+    outside = np.zeros_like(f)
+    mask = np.ones(f.shape, dtype=bool)
+    mask[w] = False
+    outside[mask] = f[mask]
+    dirichlet = np.nan_to_num(stencil.apply_operator(outside, *n, *codes, d, 0.0,
+                                                     {k: None for k in stencil.FACE_KEYS}))
+    return (f + neumann - dirichlet)[w], w
+
+
+@pytest.mark.parametrize("codes,lam", [((1, 1, 1), 0.0), ((3, 1, 3), -2.0), ((3, 3, 3), -1.5),
+                                       ((1, 3, 1), 0.0)])
+def test_19pt_emulation_solves_the_compact_scheme(codes, lam):
+    """The reference's 19-point division (dead code in the reference, no
+    outputs to pin against) is the compact fourth-order scheme: the emulated
+    solution satisfies (L19 + lambda) u = B b on the window, L19 the 19-point
+    Laplacian and B the 7-point right-hand-side filter, with the closures the
+    transforms imply."""
+    n = (12, 16, 10)
+    p = gen.random_problem(*n, *codes, lam, seed=7, dom=(0.0, 1.2, 0.0, 1.6, 0.0, 1.0))
+    d = p["dom"]
+    u = E.emulate_solver(d[0], d[1], p["nx"], p["xbc"], p["bcl"], p["bcr"],
+                         d[2], d[3], p["ny"], p["ybc"], p["bcb"], p["bct"],
+                         d[4], d[5], p["nz"], p["zbc"], p["bcf"], p["bce"], p["lam"], p["f"], stencil19=True)
+    b, w = _rhs_with_terms(p)
+    h2 = (n[0] / 1.2) ** 2
+    lhs = stencil.apply_19pt(u[w], codes, h2) + lam * u[w]
+    rhs = stencil.filter_19pt(b, codes)
+    assert np.linalg.norm(lhs - rhs) <= 1e-13 * np.linalg.norm(rhs)
