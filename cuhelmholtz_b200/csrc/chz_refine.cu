@@ -99,21 +99,24 @@ __global__ void remove_mode(double* u, BcArgs b, const double* sum, double inv_w
 // interior neighbour (the flux is in b), periodic neighbours wrap.
 //
 // A block of 32 x 8 threads marches up kResZ planes of a 32 x 8 column.  The u
-// values of each plane, with a one-point halo, are staged in shared memory by
-// cp.async, two planes ahead of the plane being computed (a ring of four
-// plane tiles); the closures are folded into the halo values as they are
-// loaded, so the stencil itself reads only shared memory.
+// values of each plane, with a one-point halo, and the f values of the
+// column are staged in shared memory by cp.async, kAhead planes ahead of the
+// plane being computed (rings of kRing plane tiles); the closures are folded
+// into the halo values as they are loaded, so the stencil itself reads only
+// shared memory.
 constexpr int kResX = 32, kResY = 8, kResZ = 32;
 constexpr int kHX = kResX + 2, kHY = kResY + 2, kHalo = kHX * kHY;
+constexpr int kAhead = 5;  // planes requested ahead of the computed one
+constexpr int kRing = 8;   // >= kAhead + 3: a load reuses the slot of plane k - 3
 
 // Source index along one axis for window-relative neighbour g (one step
 // outside the window at most): -1 when the value is 0 (Dirichlet neighbour).
 __device__ __forceinline__ int closure_index(int g, int s, int e, int n, int bc) {
     if (g >= s && g <= e) return g;
     if (g == s - 1) {
-        if (bc == 0) return n - 1;          // periodic: s = 0
+        if (bc == 0) return n - 1;             // periodic: s = 0
         if (bc == 3 || bc == 4) return s + 1;  // Neumann mirror
-        return -1;                          // Dirichlet
+        return -1;                             // Dirichlet
     }
     if (g == e + 1) {
         if (bc == 0) return 0;
@@ -123,22 +126,56 @@ __device__ __forceinline__ int closure_index(int g, int s, int e, int n, int bc)
     return -1;  // beyond the halo: never read
 }
 
-__device__ __forceinline__ void load_plane(double* tile, const double* u, const BcArgs& b, int i0, int j0, int p,
-                                           long long sy, long long sz, int tid) {
-    const int kk = closure_index(p, b.zs, b.ze, b.nz, b.zbc);
-    for (int e = tid; e < kHalo; e += kResX * kResY) {
-        const int hy = e / kHX, hx = e - hy * kHX;
-        const int ii = closure_index(i0 - 1 + hx, b.xs, b.xe, b.nx, b.xbc);
-        const int jj = closure_index(j0 - 1 + hy, b.ys, b.ye, b.ny, b.ybc);
-        const bool valid = kk >= 0 && ii >= 0 && jj >= 0;
-        const double* src = valid ? u + (long long)kk * sz + (long long)jj * sy + ii : u;
-        cp_async_elem<8>(tile + e, src, valid);
+// Per-thread copy plan of one plane tile: the (x, y) offsets of the (at most
+// two) halo entries this thread copies, or -1 when the entry is 0
+// (Dirichlet neighbour, or outside the halo); the z closure is applied per
+// plane.
+struct HaloPlan {
+    long long off[2];
+    long long foff;  // the thread's own point in f, or -1
+};
+
+__device__ __forceinline__ HaloPlan halo_plan(const BcArgs& b, int i0, int j0, long long sy, int tid) {
+    HaloPlan h;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        const int e = tid + r * kResX * kResY;
+        h.off[r] = -1;
+        if (e < kHalo) {
+            const int hy = e / kHX, hx = e - hy * kHX;
+            const int ii = closure_index(i0 - 1 + hx, b.xs, b.xe, b.nx, b.xbc);
+            const int jj = closure_index(j0 - 1 + hy, b.ys, b.ye, b.ny, b.ybc);
+            if (ii >= 0 && jj >= 0) h.off[r] = (long long)jj * sy + ii;
+        }
     }
+    const int ty = tid / kResX, tx = tid - ty * kResX;
+    const int i = i0 + tx, j = j0 + ty;
+    h.foff = (i <= b.xe && j <= b.ye) ? (long long)j * sy + i : -1;
+    return h;
+}
+
+// Issues the copies of plane p (u with halo, f of the column) and commits
+// them as one group.
+__device__ __forceinline__ void load_plane(double* tile, double* ftile, const double* u, const BcArgs& b,
+                                           const HaloPlan& h, int p, long long sz, int tid) {
+    const int kk = closure_index(p, b.zs, b.ze, b.nz, b.zbc);
+    const long long base = (long long)kk * sz;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        const int e = tid + r * kResX * kResY;
+        if (e < kHalo) {
+            const bool valid = kk >= 0 && h.off[r] >= 0;
+            cp_async_elem<8>(tile + e, valid ? u + base + h.off[r] : u, valid);
+        }
+    }
+    const bool fv = p >= b.zs && p <= b.ze && h.foff >= 0;
+    cp_async_elem<8>(ftile + tid, fv ? b.f + (long long)p * sz + h.foff : b.f, fv);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
 
 __global__ void __launch_bounds__(kResX * kResY) residual_kernel(ResidualArgs a) {
-    __shared__ __align__(16) double ring[4][kHalo];
+    __shared__ __align__(16) double ring[kRing][kHalo];
+    __shared__ __align__(16) double fring[kRing][kResX * kResY];
     const BcArgs& b = a.bc;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kResX + tx;
     const int i0 = b.xs + blockIdx.x * kResX, j0 = b.ys + blockIdx.y * kResY;
@@ -150,38 +187,40 @@ __global__ void __launch_bounds__(kResX * kResY) residual_kernel(ResidualArgs a)
     const bool side = (i == b.xs || i == b.xe || j == b.ys || j == b.ye);
     const double shift = a.shift ? *a.shift * a.inv_w : 0.0;
     double r2 = 0.0, b2 = 0.0;
-    // planes k0 - 1, k0, k0 + 1 and (prefetch) k0 + 2 in slots 0..3
-    for (int q = 0; q < 4; ++q) {
-        if (k0 - 1 + q <= k1 + 1) load_plane(ring[q], a.u, b, i0, j0, k0 - 1 + q, sy, sz, tid);
+    const HaloPlan hp = halo_plan(b, i0, j0, sy, tid);
+    // plane p lives in slot (p - k0 + 1) & (kRing - 1); planes k0 - 1 .. k0 + kAhead - 1 first
+    for (int q = 0; q < kAhead + 1; ++q) {
+        const int p = k0 - 1 + q;
+        if (p <= k1 + 1) load_plane(ring[q], fring[q], a.u, b, hp, p, sz, tid);
         else asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
-    const double* fcol = b.f + (long long)j * sy + i;
-    double fv = act ? __ldg(fcol + (long long)k0 * sz) : 0.0;
     const int c = (ty + 1) * kHX + tx + 1;
     for (int k = k0; k <= k1; ++k) {
-        const int q = k - k0;  // slot of plane k - 1 is q & 3
-        // planes k - 1, k, k + 1 have landed (plane k + 2 may still be in flight)
-        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-        __syncthreads();
-        const double fnext = (act && k + 1 <= k1) ? __ldg(fcol + (long long)(k + 1) * sz) : 0.0;
+        const int q = k - k0;  // slot of plane k - 1 is q & (kRing - 1)
+        // planes up to k + 1 have landed (planes k + 2 .. k + kAhead - 1 may be in flight)
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(kAhead - 2) : "memory");
+        __syncthreads();  // also: every thread is done with plane k - 3's slot
+        {
+            const int p = k + kAhead;
+            const int sl = (q + kAhead + 1) & (kRing - 1);
+            if (p <= k1 + 1) load_plane(ring[sl], fring[sl], a.u, b, hp, p, sz, tid);
+            else asm volatile("cp.async.commit_group;\n" ::: "memory");
+        }
         if (act) {
-            const double* lo = ring[q & 3];
-            const double* mid = ring[(q + 1) & 3];
-            const double* hi = ring[(q + 2) & 3];
+            const double* lo = ring[q & (kRing - 1)];
+            const double* mid = ring[(q + 1) & (kRing - 1)];
+            const double* hi = ring[(q + 2) & (kRing - 1)];
             const double uc = mid[c];
             const double au = (((mid[c - 1] - 2.0 * uc + mid[c + 1]) * b.dx2 +
                                 (mid[c - kHX] - 2.0 * uc + mid[c + kHX]) * b.dy2) +
                                (lo[c] - 2.0 * uc + hi[c]) * b.dz2) + a.lambda * uc;
+            const double fv = fring[(q + 1) & (kRing - 1)][tid];
             const double bv = (side || k == b.zs || k == b.ze) ? bc_terms(fv, b, i, j, k) : fv;
             const double rv = (bv - au) - shift;
             a.r[k * a.rz + j * a.ry + i] = (float)rv;
             r2 += rv * rv;
             b2 += bv * bv;
         }
-        fv = fnext;
-        __syncthreads();  // slot of plane k - 1 is free
-        if (k + 3 <= k1 + 1) load_plane(ring[q & 3], a.u, b, i0, j0, k + 3, sy, sz, tid);
-        else asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     if (a.sums) {
