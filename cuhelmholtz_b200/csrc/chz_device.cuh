@@ -329,10 +329,22 @@ __host__ __device__ __forceinline__ void kind_out_window(int kind, int N, int& l
 //   DCT1: V[m] = x[2m] + i (x[2m-1] - x[2m+1]), V[0] = x[0], V[M] = x[N]
 //   DST1: V[m] = (x[2m+1] - x[2m-1]) - i x[2m], V[0] = 2 x[1], V[M] = -2 x[N-1]
 // ---------------------------------------------------------------------------
+// Real view of one line: entry l at R[l * PR + c].
+template <typename T>
+struct StridedView {
+    const T* __restrict__ R;
+    int PR, c;
+    __device__ __forceinline__ T operator()(int l) const { return R[l * PR + c]; }
+};
+
 template <typename T>
 __device__ __forceinline__ C2<T> inv_spectrum(int kind, const T* __restrict__ R, int PR, int c,
-                                              int k, int N, int M, const LineTables<T>& tb) {
-#define X(l) R[(l) * PR + c]
+                                              int k, int N, int M, const LineTables<T>& tb);
+
+// The same on any real-view accessor V (entry l of the line: V(l)).
+template <typename T, typename V>
+__device__ __forceinline__ C2<T> inv_spectrum_v(int kind, const V& X, int k, int N, int M,
+                                                const LineTables<T>& tb) {
     switch (kind) {
         case kC2R: {
             if (k == 0 || k == M) return mk<T>(X(2 * k), T(0));
@@ -366,18 +378,28 @@ __device__ __forceinline__ C2<T> inv_spectrum(int kind, const T* __restrict__ R,
             return mk<T>(X(2 * k + 1) - X(2 * k - 1), -X(2 * k));
         }
     }
-#undef X
+}
+
+template <typename T>
+__device__ __forceinline__ C2<T> inv_spectrum(int kind, const T* __restrict__ R, int PR, int c,
+                                              int k, int N, int M, const LineTables<T>& tb) {
+    return inv_spectrum_v<T>(kind, StridedView<T>{R, PR, c}, k, N, M, tb);
+}
+
+template <typename T, typename V>
+__device__ __forceinline__ T fwd_gather_v(int kind, const V& X, int j, int N, int M) {
+    switch (kind) {
+        case kR2C: return X(j);
+        case kDCT2: return (j < M) ? X(2 * j) : X(2 * N - 1 - 2 * j);
+        default:  // kDST2
+            return (j < M) ? X(2 * j + 1) : -X(2 * N - 2 * j);
+    }
 }
 
 template <typename T>
 __device__ __forceinline__ T fwd_gather(int kind, const T* __restrict__ R, int PR, int c, int j,
                                         int N, int M) {
-    switch (kind) {
-        case kR2C: return R[j * PR + c];
-        case kDCT2: return (j < M) ? R[(2 * j) * PR + c] : R[(2 * N - 1 - 2 * j) * PR + c];
-        default:  // kDST2
-            return (j < M) ? R[(2 * j + 1) * PR + c] : -R[(2 * N - 2 * j) * PR + c];
-    }
+    return fwd_gather_v<T>(kind, StridedView<T>{R, PR, c}, j, N, M);
 }
 
 template <typename T>

@@ -51,6 +51,12 @@ struct LineCfg {
         if constexpr (BAR == 0) __syncthreads();
         else asm volatile("bar.sync %0, %1;\n" ::"n"(BAR), "n"(NT) : "memory");
     }
+    // real view of line c: reader(buf, c)(l) = buf[l * PR + c]; complex view Z[zi(m, c)]
+    template <typename T>
+    __device__ static __forceinline__ StridedView<T> reader(const T* buf, int c) {
+        return StridedView<T>{buf, PR, c};
+    }
+    __device__ static __forceinline__ int zi(int m, int c) { return m * W + c; }
 };
 
 // The persistent cp.async kernel: 128 threads, odd pitch W + 1 (conflict-free
@@ -144,14 +150,14 @@ __device__ __forceinline__ void stage_compute(C2<T>* v, int slot, const C2<T>* _
 
 // Complex value A[n] fed to the FFT, from the real view (pre step); the kind
 // is a compile-time constant so the gathers fold to fixed offsets.
-template <typename T, int KIND, int M, int PR>
-__device__ __forceinline__ C2<T> pre_value(const T* __restrict__ Rv, int c, int n, const LineTables<T>& tb) {
+template <typename T, int KIND, int M, typename V>
+__device__ __forceinline__ C2<T> pre_value(const V& X, int n, const LineTables<T>& tb) {
     constexpr int N = 2 * M;
     if constexpr (KIND == kR2C || KIND == kDCT2 || KIND == kDST2) {
-        return mk<T>(fwd_gather<T>(KIND, Rv, PR, c, 2 * n, N, M), fwd_gather<T>(KIND, Rv, PR, c, 2 * n + 1, N, M));
+        return mk<T>(fwd_gather_v<T>(KIND, X, 2 * n, N, M), fwd_gather_v<T>(KIND, X, 2 * n + 1, N, M));
     } else {
-        const C2<T> vk = inv_spectrum<T>(KIND, Rv, PR, c, n, N, M, tb);
-        const C2<T> vm = inv_spectrum<T>(KIND, Rv, PR, c, M - n, N, M, tb);
+        const C2<T> vk = inv_spectrum_v<T>(KIND, X, n, N, M, tb);
+        const C2<T> vm = inv_spectrum_v<T>(KIND, X, M - n, N, M, tb);
         const C2<T> wk = ldtw<T>(tb.twN + n);
         const C2<T> e = cadd<T>(vk, cconj<T>(vm));
         const C2<T> o = cmul<T>(cconj<T>(wk), csub<T>(vk, cconj<T>(vm)));
@@ -216,8 +222,9 @@ template <typename T, typename CF, int KIND, typename SINK>
 __device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot, const LineTables<T>& tb,
                                                 const SINK& sink) {
     constexpr int M = CF::M;
-    constexpr int W = CF::W, PR = CF::PR, N = CF::N, P = CF::P;
+    constexpr int W = CF::W, N = CF::N, P = CF::P;
     constexpr bool FWD = (KIND == kR2C || KIND == kDCT2 || KIND == kDST2);
+    const auto X = CF::reader(static_cast<const T*>(buf), c);
     C2<T>* Z = reinterpret_cast<C2<T>*>(buf);
     C2<T> v[kR];
 
@@ -225,7 +232,7 @@ __device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot,
     if constexpr (KIND == kDCT1) {
         T acc = T(0);
 #pragma unroll
-        for (int q = 0; q < M / P; ++q) acc += buf[(2 * (slot + q * P) + 1) * PR + c];
+        for (int q = 0; q < M / P; ++q) acc += X(2 * (slot + q * P) + 1);
         red[slot * W + c] = acc;
     }
 
@@ -233,7 +240,7 @@ __device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot,
     {
         using BF = Bfly<M, 0>;
 #pragma unroll
-        for (int k = 0; k < kR; ++k) v[k] = pre_value<T, KIND, M, PR>(buf, c, BF::in_idx(slot, 0, k), tb);
+        for (int k = 0; k < kR; ++k) v[k] = pre_value<T, KIND, M>(X, BF::in_idx(slot, 0, k), tb);
         CF::sync();
         stage_compute<T, M, 0>(v, slot, tb.twM);
     }
@@ -244,12 +251,12 @@ __device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot,
         using PB = Bfly<M, S - 1>;                                                            \
         _Pragma("unroll") for (int b = 0; b < PB::B; ++b)                                     \
             _Pragma("unroll") for (int k = 0; k < PB::r; ++k)                                 \
-                Z[PB::out_idx(slot, b, k) * W + c] = v[b * PB::r + k];                        \
+                Z[CF::zi(PB::out_idx(slot, b, k), c)] = v[b * PB::r + k];                        \
         CF::sync();                                                                      \
         using BF = Bfly<M, S>;                                                                \
         _Pragma("unroll") for (int b = 0; b < BF::B; ++b)                                     \
             _Pragma("unroll") for (int k = 0; k < BF::r; ++k)                                 \
-                v[b * BF::r + k] = Z[BF::in_idx(slot, b, k) * W + c];                         \
+                v[b * BF::r + k] = Z[CF::zi(BF::in_idx(slot, b, k), c)];                         \
         CF::sync();                                                                      \
         stage_compute<T, M, S>(v, slot, tb.twM);                                              \
     }
@@ -264,7 +271,7 @@ __device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot,
 #pragma unroll
         for (int b = 0; b < LB::B; ++b)
 #pragma unroll
-            for (int k = 0; k < LB::r; ++k) Z[LB::out_idx(slot, b, k) * W + c] = v[b * LB::r + k];
+            for (int k = 0; k < LB::r; ++k) Z[CF::zi(LB::out_idx(slot, b, k), c)] = v[b * LB::r + k];
         CF::sync();
     }
     if constexpr (FWD) {
@@ -276,7 +283,7 @@ __device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot,
             for (int k = 0; k < LB::r; ++k) {
                 const int m = LB::out_idx(slot, b, k);
                 const C2<T> zk = v[b * LB::r + k];
-                const C2<T> zm = Z[((M - m) & (M - 1)) * W + c];
+                const C2<T> zm = Z[CF::zi((M - m) & (M - 1), c)];
                 const C2<T> wk = ldtw<T>(tb.twN + m);
                 const C2<T> e = cadd<T>(zk, cconj<T>(zm));
                 const C2<T> o = cmul<T>(wk, csub<T>(zk, cconj<T>(zm)));
@@ -337,12 +344,12 @@ __device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot,
                         oe = T(0);
                     }
                 } else {
-                    const T pe = Z[(M - m) * W + c].x;  // v[N-2m]
+                    const T pe = Z[CF::zi(M - m, c)].x;  // v[N-2m]
                     const T is4 = ldr<T>(tb.inv4sin + (2 * m <= M ? 2 * m : N - 2 * m));
                     if constexpr (KIND == kDCT1) oe = ((ve + pe) * T(0.5) - (ve - pe) * is4) * T(0.5);
                     else oe = ((ve + pe) * is4 + (ve - pe) * T(0.5)) * T(0.5);
                 }
-                const T po = -Z[(M - m - 1) * W + c].y;  // v[N-2m-1]
+                const T po = -Z[CF::zi(M - m - 1, c)].y;  // v[N-2m-1]
                 const int ko = 2 * m + 1;
                 const T is4o = ldr<T>(tb.inv4sin + (ko <= M ? ko : N - ko));
                 T oo;

@@ -330,10 +330,30 @@ static int try_tma(const void* in, void* out, const PassArgs& a, const DeviceLin
     }
 }
 
+namespace xtma {
+template <int M>
+int launch_xtma_kind(int kind, int kind2, const void* in, void* out, const PassArgs& a,
+                     const LineTables<double>& tb, int nv, cudaStream_t stream, const char* label);
+}  // namespace xtma
+
+// FP64 contiguous passes of N = 512 whose input and output rows are both
+// 16-byte aligned (do_transform's padded arrays) go to the TMA-pipelined
+// contiguous kernel; -1 when it does not take the pass.
+static int try_xtma(const void* in, void* out, const PassArgs& a, const DeviceLineTables& tb, int nv,
+                    cudaStream_t stream, const char* label) {
+    if (a.acc || a.kind2 >= 0 || tb.M != 256) return -1;
+    const LineTables<double> t = to_tables<double>(tb);
+    return xtma::launch_xtma_kind<256>(a.kind, a.kind2, in, out, a, t, nv, stream, label);
+}
+
 int launch_line_pass(int is_double, int in_type, int out_type, bool contig, const void* in,
                      void* out, const PassArgs& a, const DeviceLineTables& tb, const LineGeom& g,
                      int nv, cudaStream_t stream, const char* label) {
     const int family = g_force_generic.load(std::memory_order_relaxed);
+    if (contig && family == 0 && is_double && in_type == kIoF64 && out_type == kIoF64) {
+        const int rc = try_xtma(in, out, a, tb, nv, stream, label);
+        if (rc != -1) return rc;
+    }
     if (!contig && family == 0 && in_type == out_type) {
         const int rc = is_double ? try_tma<double>(in, out, a, tb, nv, stream, label)
                                  : try_tma<float>(in, out, a, tb, nv, stream, label);

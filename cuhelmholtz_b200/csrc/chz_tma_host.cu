@@ -55,6 +55,26 @@ bool encode_map(CUtensorMap* map, bool is_double, const void* base, const unsign
     return r == CUDA_SUCCESS;
 }
 
+// 3-D FP64 map with the 128-byte swizzle (the contiguous-pass tiles).
+bool encode_map_swz(CUtensorMap* map, const void* base, const unsigned long long dims[3],
+                    const unsigned long long strides[2], const unsigned box[3]) {
+    EncodeTiledFn fn = encoder();
+    if (!fn) return false;
+    for (int i = 0; i < 3; ++i)
+        if (dims[i] < 1 || dims[i] > (1ull << 32) || box[i] < 1 || box[i] > 256) return false;
+    for (int i = 0; i < 2; ++i)
+        if (strides[i] % 16 || strides[i] >= (1ull << 40)) return false;
+    if (box[0] * 8 != 128 || (reinterpret_cast<uintptr_t>(base) & 15)) return false;
+    const cuuint64_t d[3] = {dims[0], dims[1], dims[2]};
+    const cuuint64_t s[2] = {strides[0], strides[1]};
+    const cuuint32_t b[3] = {box[0], box[1], box[2]};
+    const cuuint32_t e[3] = {1, 1, 1};
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(base), d, s, b, e,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 int* device_flags() {
     static std::atomic<int*> cached[64];
     int dev = 0;
