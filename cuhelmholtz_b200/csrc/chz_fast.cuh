@@ -479,7 +479,13 @@ fast_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tg, int ntx, int ntil
 
     const int t = threadIdx.x;
     const int c = t % W;
-    const int slot = t / W;
+    // slots of a warp: with 8 lines a tile (N = 512) the contiguous passes give
+    // warp w the slots w, w + 4, w + 8, w + 12 -- their real-view rows then
+    // start 0 / 8 (or 0 / 4 / 8 / 12) 8-byte words apart mod 16 at pitch 9, so
+    // the 32 accesses of an instruction hit each bank pair exactly twice (four
+    // consecutive slots collide 4-way); elsewhere consecutive slots
+    constexpr bool spread = CONTIG && W == 8;
+    const int slot = spread ? (t >> 5) + (kNT / 32) * ((t & 31) / W) : t / W;
     if ((int)blockIdx.x >= ntiles) return;
 
     // stage the line tables in shared memory once (the CTA is persistent)
