@@ -11,5 +11,6 @@ from .api import (  # noqa: F401
     solve_problem, workspace_size,
 )
 from ._lib import lib, library_path  # noqa: F401
+from .pipeline import HostPipeline  # noqa: F401
 
 __version__ = "0.1.0"
