@@ -39,6 +39,14 @@ struct TileW {
 template <typename T, int M>
 using TCfg = LineCfg<M, TileW<T>::W, TileW<T>::W, 1>;
 
+// The DCT/DST tables (tw4N, inv4sin) are staged in shared memory only for
+// passes that use them.
+template <int KIND, int KIND2>
+struct UsesDctTables {
+    static constexpr bool dft(int k) { return k == kR2C || k == kC2R; }
+    static constexpr bool value = !dft(KIND) || (KIND2 >= 0 && !dft(KIND2));
+};
+
 constexpr int kStages = 3;
 
 // Host-computed geometry of one pass.
@@ -108,7 +116,7 @@ __device__ __forceinline__ void tma_store(const CUtensorMap* map, int c0, int c1
 }
 
 // Shared-memory carve-up (byte offsets).
-template <typename T, int M, bool FUSED>
+template <typename T, int M, bool FUSED, bool DCTTAB = true>
 struct TmaSmem {
     using CF = TCfg<T, M>;
     __host__ __device__ static constexpr size_t al(size_t b, size_t a) { return (b + a - 1) / a * a; }
@@ -116,8 +124,12 @@ struct TmaSmem {
     __host__ __device__ static size_t twM(int rows_buf) { return al(kStages * stage_bytes(rows_buf), 128); }
     __host__ __device__ static size_t twN(int rows_buf) { return twM(rows_buf) + sizeof(C2<T>) * M; }
     __host__ __device__ static size_t tw4N(int rows_buf) { return twN(rows_buf) + sizeof(C2<T>) * (M + 1); }
-    __host__ __device__ static size_t inv4sin(int rows_buf) { return tw4N(rows_buf) + sizeof(C2<T>) * (M + 1); }
-    __host__ __device__ static size_t ez(int rows_buf) { return al(inv4sin(rows_buf) + sizeof(T) * (M + 1), 16); }
+    __host__ __device__ static size_t inv4sin(int rows_buf) {
+        return tw4N(rows_buf) + (DCTTAB ? sizeof(C2<T>) * (M + 1) : 0);
+    }
+    __host__ __device__ static size_t ez(int rows_buf) {
+        return al(inv4sin(rows_buf) + (DCTTAB ? sizeof(T) * (M + 1) : 0), 16);
+    }
     __host__ __device__ static size_t red(int rows_buf) {
         return al(ez(rows_buf) + (FUSED ? sizeof(double) * (2 * M + 2) : 0), 16);
     }
@@ -131,7 +143,8 @@ __global__ void __launch_bounds__(TCfg<T, M>::NT + 32, 1)
 tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUtensorMap stmap, PassArgs a,
          LineTables<T> tg, TmaGeom g, int ntx, int ntiles, int* flags) {
     using CF = TCfg<T, M>;
-    using SL = TmaSmem<T, M, (KIND2 >= 0)>;
+    constexpr bool DCTTAB = UsesDctTables<KIND, KIND2>::value;
+    using SL = TmaSmem<T, M, (KIND2 >= 0), DCTTAB>;
     constexpr int W = CF::W, PR = CF::PR, NT = CF::NT, N = CF::N;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int t = threadIdx.x;
@@ -156,13 +169,17 @@ tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUte
         for (int i = t; i < M; i += blockDim.x) sM[i] = tg.twM[i];
         for (int i = t; i <= M; i += blockDim.x) {
             sN[i] = tg.twN[i];
-            s4[i] = tg.tw4N[i];
-            sI[i] = tg.inv4sin[i];
+            if constexpr (DCTTAB) {
+                s4[i] = tg.tw4N[i];
+                sI[i] = tg.inv4sin[i];
+            }
         }
         tb.twM = sM;
         tb.twN = sN;
-        tb.tw4N = s4;
-        tb.inv4sin = sI;
+        if constexpr (DCTTAB) {
+            tb.tw4N = s4;
+            tb.inv4sin = sI;
+        }
     }
     double* ez_s = reinterpret_cast<double*>(smem_raw + SL::ez(rb));
     if constexpr (KIND2 >= 0) {

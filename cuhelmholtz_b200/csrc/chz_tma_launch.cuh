@@ -59,7 +59,7 @@ int launch_one(const T* in, T* out, const PassArgs& a, const LineTables<T>& tb, 
     g.rows_buf = (rows + 7) & ~7;
     g.tx_bytes = (unsigned)(g.ld_nch * g.ld_box * W * ES);
 
-    using SL = TmaSmem<T, M, (K2 >= 0)>;
+    using SL = TmaSmem<T, M, (K2 >= 0), UsesDctTables<KIND, K2>::value>;
     const size_t smem = SL::total(g.rows_buf);
     if ((long long)smem > (long long)max_optin_smem()) return -1;
 

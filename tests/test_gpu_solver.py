@@ -153,3 +153,17 @@ def test_bad_boundary_code_raises():
     with pytest.raises(api.CHZError):
         api.cuda_helmholtz_solver(0, 1, 8, 7, None, None, 0, 1, 8, 1, None, None, 0, 1, 8, 1,
                                   None, None, -1.0, f)
+
+
+@pytest.mark.parametrize("dims,bcs,lam", [
+    ((40, 24, 512), (3, 4, 0), -1.0),
+    ((18, 10, 512), (1, 2, 0), -2.5),    # x window starts at 1: map column 0 rounded down
+    ((24, 40, 512), (0, 0, 0), 0.0),     # singular: zero mode removed in the z pass
+    ((36, 20, 512), (3, 3, 0), 0.0),
+    ((16, 16, 512), (4, 1, 0), -7.0),
+])
+def test_periodic_z_512_vs_oracle(dims, bcs, lam):
+    """Periodic z with N = 512: the fused forward / division / inverse z pass
+    of the TMA kernel on 16-line tiles, the singular cases included."""
+    p = gen.random_problem(*dims, *bcs, lam, seed=7 + sum(bcs))
+    assert rel(gpu_solve(p), emulated(p)) < TOL
