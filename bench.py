@@ -187,6 +187,52 @@ def cpu_baseline_single(p):
                       "FISHPACK hw3crt via the reference's solver_3d, 1 thread"}
 
 
+# forward transform kind of each boundary code (the solver's first passes)
+FORWARD_KIND = {0: 6, 1: 3, 2: 5, 3: 0, 4: 2}
+# the standalone transform of the 128^3 configuration: DST-I, DST-II, DFT (in place)
+TRANSFORM_KINDS = {"helmholtz_fp64_128": (3, 4, 6)}
+
+
+def time_transform(chz, name, nx, ny, nz, bcs, steps, warmup, world, peak):
+    """do_transform timed alone: in place on cubic grids, out of place
+    otherwise (the reference's rule), FP64, kinds = the workload's forward
+    kinds.  Enough arrays are cycled that the working set exceeds L2."""
+    import numpy as np
+    import torch
+    kinds = TRANSFORM_KINDS.get(name, tuple(FORWARD_KIND[b] for b in bcs))
+    n = chz.padded_numel(nx, ny, nz)
+    inplace = nx == ny == nz
+    per = n * 8 * (1 if inplace else 2)
+    count = max(2, -(-(256 << 20) // per))
+    rng = np.random.default_rng(17)
+    base = torch.from_numpy(rng.standard_normal(n)).cuda()
+    bufs = [base.clone() for _ in range(count)]
+    outs = [None if inplace else torch.empty_like(base) for _ in range(count)]
+
+    def run(i):
+        chz.do_transform(bufs[i], outs[i], nx, ny, nz, *kinds)
+
+    for w in range(max(warmup, 1)):
+        for i in range(count):
+            run(i)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(steps):
+        run(k % count)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), world, "cuda") / steps
+    model_bytes = 48 * nx * ny * nz
+    gbs = model_bytes / (ms / 1000.0) / 1e9
+    return {"kinds": [chz.KIND_NAMES[k] for k in kinds], "inplace": inplace, "value": world * 1000.0 / ms,
+            "unit": "transforms/s", "ms_per_transform": ms, "model_bytes": model_bytes,
+            "model": "48 B per point (3 passes x 8 B read + 8 B written), points = NX*NY*NZ",
+            "model_gbs": gbs, "frac_of_peak": gbs / peak, "arrays_cycled": count}
+
+
 def run_reference_arm(args):
     """The reference's CPU implementation of the path on the host cores:
     concurrent single-threaded hw3crt processes (hw3crt is serial)."""
@@ -369,6 +415,12 @@ def run_ours(args):
     dom_k = max(line_labels, key=lambda k: tr[k][1]) if line_labels else None
     dom_gbs = per_pass[dom_k]["gbs"] if dom_k else None
 
+    # ---- the transform alone: do_transform with the workload's forward kinds ----
+    transform = None
+    if args.transform_steps > 0:
+        transform = time_transform(chz, name, nx, ny, nz, (xbc, ybc, zbc), args.transform_steps,
+                                   args.warmup, world, peak)
+
     # ---- FP32 transforms + FP64 refinement on the same problems ----
     refine = None
     if args.refine_corrections >= 0:
@@ -498,6 +550,7 @@ def run_ours(args):
         "clocks": clocks,
         "rel_residual": rel_residual,
         "fp32_refine": refine,
+        "transform": transform,
     }
     print(json.dumps(line))
     return 0
@@ -589,6 +642,8 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--batch", type=int, default=8, help="solves per step (separate arrays)")
     ap.add_argument("--e2e-steps", type=int, default=8)
+    ap.add_argument("--transform-steps", type=int, default=20,
+                    help="timed do_transform calls (0 skips the transform leg)")
     ap.add_argument("--ref-procs", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--check", action="store_true", help="report the residual of the solve")
