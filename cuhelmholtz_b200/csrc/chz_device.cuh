@@ -39,6 +39,18 @@ __device__ __forceinline__ C2<T> cmul_negi(C2<T> a) { return mk<T>(a.y, -a.x); }
 template <typename T>
 __device__ __forceinline__ C2<T> cmul_i(C2<T> a) { return mk<T>(-a.y, a.x); }
 
+// 1/d: the hardware's approximate FP64 reciprocal (about 23 good bits)
+// refined by two Newton-Raphson steps r <- r + r (1 - d r), each of which
+// squares the relative error (2^-23 -> 2^-46 -> below double rounding).
+__device__ __forceinline__ double recip_nr(double d) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+    double e = fma(-d, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-d, r, 1.0);
+    return fma(r, e, r);
+}
+
 // Table reads: plain loads, so the same code reads tables in global memory
 // (generic kernel) or staged in shared memory (register-resident kernels).
 template <typename T>
@@ -179,13 +191,17 @@ __device__ __forceinline__ void fft_stage(const C2<T>* __restrict__ src, C2<T>* 
     const int nb = M / R;
     const int total = nb << log2W;
     const int tstep = M / (Ns * R);
+    // idx advances by nthr (a multiple of W): c stays, j advances by jstep,
+    // and p = j mod Ns is carried along instead of divided out per butterfly
+    const int c = tid & (W - 1);
+    const int jstep = nthr >> log2W;
+    const int pstep = jstep % Ns;
+    int p = (tid >> log2W) % Ns;
     for (int idx = tid; idx < total; idx += nthr) {
-        const int c = idx & (W - 1);
         const int j = idx >> log2W;
         C2<T> v[R];
 #pragma unroll
         for (int k = 0; k < R; ++k) v[k] = src[((j + k * nb) << log2W) + c];
-        const int p = j % Ns;
         if (Ns > 1) {
 #pragma unroll
             for (int k = 1; k < R; ++k) v[k] = cmul<T>(v[k], ldtw<T>(twM + p * k * tstep));
@@ -194,6 +210,8 @@ __device__ __forceinline__ void fft_stage(const C2<T>* __restrict__ src, C2<T>* 
         const int base = (j - p) * R + p;
 #pragma unroll
         for (int k = 0; k < R; ++k) dst[((base + k * Ns) << log2W) + c] = v[k];
+        p += pstep;
+        if (p >= Ns) p -= Ns;
     }
 }
 

@@ -203,17 +203,7 @@ struct OutSink {
         Rv[l * PR + c] = re;
         Rv[(l + 1) * PR + c] = im;
     }
-    // 1/d: the hardware's approximate FP64 reciprocal (about 23 good bits)
-    // refined by two Newton-Raphson steps r <- r + r (1 - d r), each of which
-    // squares the relative error (2^-23 -> 2^-46 -> below double rounding).
-    __device__ static __forceinline__ double recip(double d) {
-        double r;
-        asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
-        double e = fma(-d, r, 1.0);
-        r = fma(r, e, r);
-        e = fma(-d, r, 1.0);
-        return fma(r, e, r);
-    }
+    __device__ static __forceinline__ double recip(double d) { return recip_nr(d); }
 };
 
 // One complete real transform of the W lines held in `buf` (real view in,

@@ -116,20 +116,23 @@ __device__ __forceinline__ void line_pass_tile(const TI* in, TO* out, const Pass
         __syncthreads();
         if (rep == 0 && a.kind2 >= 0) {
             if (a.has_div) {
+                // idx advances by nthr (a multiple of W): each thread keeps
+                // one column c, so ex[i] + ey[j] is read once
                 const DivArgs& d = a.dv;
                 const int len = d.hi - d.lo + 1;
                 const int total = len << log2W;
-                for (int idx = tid; idx < total; idx += nthr) {
-                    const int c = idx & (W - 1);
-                    const int l = d.lo + (idx >> log2W);
-                    if (c >= nl) continue;
-                    const int i = ub + c;  // x entry (u)
-                    const int j = v;       // y entry (v)
-                    const double den = ((__ldg(d.ex + i) + __ldg(d.ey + j)) + __ldg(d.ez + l)) + d.lambda;
-                    double eig = 1.0 / den;
-                    if (d.perturb && i <= d.xz_hi && j <= d.yz_hi && l <= d.zz_hi) eig = 0.0;
-                    T& r = rout[l * PR + c];
-                    r = (T)((double)r * eig);
+                const int c = tid & (W - 1);
+                const int i = ub + c;  // x entry (u)
+                const int j = v;       // y entry (v)
+                if (c < nl) {
+                    const double exy = __ldg(d.ex + i) + __ldg(d.ey + j);
+                    const int zmax = (d.perturb && i <= d.xz_hi && j <= d.yz_hi) ? d.zz_hi : -1;
+                    for (int idx = tid; idx < total; idx += nthr) {
+                        const int l = d.lo + (idx >> log2W);
+                        const double eig = l <= zmax ? 0.0 : recip_nr((exy + __ldg(d.ez + l)) + d.lambda);
+                        T& r = rout[l * PR + c];
+                        r = (T)((double)r * eig);
+                    }
                 }
                 __syncthreads();
             }
