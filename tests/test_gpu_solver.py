@@ -167,3 +167,18 @@ def test_periodic_z_512_vs_oracle(dims, bcs, lam):
     of the TMA kernel on 16-line tiles, the singular cases included."""
     p = gen.random_problem(*dims, *bcs, lam, seed=7 + sum(bcs))
     assert rel(gpu_solve(p), emulated(p)) < TOL
+
+
+@pytest.mark.parametrize("xy", list(itertools.product(range(5), repeat=2)))
+def test_config2_all_25_pairs_manufactured(xy):
+    """The rectangular configuration's sweep: 256 x 192 x 320, every (x, y)
+    code pair with z = 3 (the out-of-place, non-cubic path; the 192- and
+    320-point axes on the generic mixed-radix kernel), lambda from the
+    configuration's range.  f = A_h u, so the solve must return u itself."""
+    import numpy as _np
+    xbc, ybc = xy
+    lam = float(_np.random.default_rng(1000 + 5 * xbc + ybc).uniform(-50.0, -0.5))
+    p = gen.manufactured_problem(256, 192, 320, xbc, ybc, 3, lam, seed=40 + 5 * xbc + ybc)
+    u = gpu_solve(p)
+    w = stencil.window_slices(256, 192, 320, xbc, ybc, 3)
+    assert rel(u[w], p["u_exact"][w]) < TOL
