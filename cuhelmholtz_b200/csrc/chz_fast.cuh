@@ -203,6 +203,17 @@ struct OutSink {
         Rv[l * PR + c] = re;
         Rv[(l + 1) * PR + c] = im;
     }
+    // put_pair's division applied to a bin held in registers.
+    __device__ __forceinline__ void div_pair(int l, C2<T>& v) const {
+        if (l >= dlo && l + 1 <= dhi) {
+            const double e = eig(l);
+            v.x = (T)((double)v.x * e);
+            v.y = (T)((double)v.y * e);
+        } else {
+            if (l >= dlo && l <= dhi) v.x = (T)((double)v.x * eig(l));
+            if (l + 1 >= dlo && l + 1 <= dhi) v.y = (T)((double)v.y * eig(l + 1));
+        }
+    }
     __device__ static __forceinline__ double recip(double d) { return recip_nr(d); }
 };
 

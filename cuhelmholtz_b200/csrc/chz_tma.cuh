@@ -14,7 +14,10 @@
 //
 // Every entry of a 128-byte row is read or written by the W threads of one
 // slot at once, so all shared accesses of the real view are bank-conflict
-// free; the complex exchange view Z[m * W + c] is two rows per entry.
+// free; the complex exchange view Z[m * W + c] is two rows per entry.  The
+// fused z pass of the solver at N = 512 (forward real DFT, division, inverse)
+// keeps the spectrum in registers between the two transforms
+// (r2c_div_c2r_regs).
 //
 // Waits are bounded: a wait that runs out sets a flag that the host can read
 // (chz_debug_flags) and the thread carries on, so the kernel always ends.
@@ -113,6 +116,130 @@ __device__ __forceinline__ void tma_store(const CUtensorMap* map, int c0, int c1
                      reinterpret_cast<uint64_t>(map)),
                  "r"(c0), "r"(c1), "r"(c2), "r"(saddr(src))
                  : "memory");
+}
+
+// The fused forward / division / inverse pass of N = 512 lines (M = 256, two
+// radix-16 stages) with the spectrum kept in registers.  After the forward
+// stages thread `slot` holds bins m = slot + 16 k; the split, the division and
+// the inverse's pre step need each bin with its partner M - m, held by slot
+// 16 - slot.  Slots are paired in warps (paired_slot): warp w >= 1 holds w
+// and 16 - w, warp 0 the self-paired 0 and 8.  Each pair (m, M - m) is
+// finished once: a thread of warps 1-7 takes the partner's bin of its k < 8 by
+// shuffle, produces the inverse inputs of both bins, keeps its own and hands
+// the partner its, so the spectrum never returns to shared memory.
+template <typename T, int M, int WT, int KIND, int KIND2>
+struct RegSpectrum {
+    static constexpr bool value = M == 256 && WT == 16 && KIND == kR2C && KIND2 == kC2R;
+};
+
+__device__ __forceinline__ int paired_slot(int t) {
+    const int w = t >> 5, h = (t >> 4) & 1;
+    return w == 0 ? 8 * h : (h ? 16 - w : w);
+}
+
+template <typename T, typename CF, typename DSINK>
+__device__ __forceinline__ void r2c_div_c2r_regs(T* buf, int c, int slot, bool partner_in_warp,
+                                                 const LineTables<T>& tb, const DSINK& dv) {
+    constexpr int M = CF::M, N = CF::N, PR = CF::PR;
+    static_assert(M == 256 && CF::W == 16 && CF::P == 16, "M = 256, 16-line tiles");
+    using B0 = fast::Bfly<M, 0>;
+    using B1 = fast::Bfly<M, 1>;
+    constexpr int R = fast::kR;
+    const auto X = CF::reader(static_cast<const T*>(buf), c);
+    C2<T>* Z = reinterpret_cast<C2<T>*>(buf);
+    C2<T> v[R];
+
+    // forward: stage 0 with the pre step in the reads, exchange, stage 1
+#pragma unroll
+    for (int k = 0; k < R; ++k) v[k] = fast::pre_value<T, kR2C, M>(X, B0::in_idx(slot, 0, k), tb);
+    CF::sync();
+    fast::stage_compute<T, M, 0>(v, slot, tb.twM);
+#pragma unroll
+    for (int k = 0; k < R; ++k) Z[CF::zi(B0::out_idx(slot, 0, k), c)] = v[k];
+    CF::sync();
+#pragma unroll
+    for (int k = 0; k < R; ++k) v[k] = Z[CF::zi(B1::in_idx(slot, 0, k), c)];
+    CF::sync();
+    fast::stage_compute<T, M, 1>(v, slot, tb.twM);
+
+    // Pair (m, M - m) from Z[m] = zk, Z[M - m] = zm: the R2C split gives X[m]
+    // and X[M - m] (w^(M-m) = -conj w^m), each is divided by its eigenvalue,
+    // and the C2R pre step gives the inverse inputs at m (o1) and M - m (o2,
+    // the conjugate sums of o1's).  m = 0 pairs bin 0 with the Nyquist bin M.
+    auto pair = [&](int m, C2<T> zk, C2<T> zm, C2<T>& o1, C2<T>& o2) {
+        const C2<T> wk = ldtw<T>(tb.twN + m);
+        const C2<T> e = cadd<T>(zk, cconj<T>(zm));
+        const C2<T> od = cmul<T>(wk, csub<T>(zk, cconj<T>(zm)));
+        C2<T> a = mk<T>(T(0.5) * (e.x + od.y), T(0.5) * (e.y - od.x));    // X[m]
+        C2<T> b = mk<T>(T(0.5) * (e.x - od.y), T(-0.5) * (e.y + od.x));   // X[M - m]
+        int lb = N - 2 * m;
+        if (m == 0) {
+            a = mk<T>(zk.x + zk.y, T(0));
+            b = mk<T>(zk.x - zk.y, T(0));
+            lb = N;
+        }
+        dv.div_pair(2 * m, a);
+        dv.div_pair(lb, b);
+        const C2<T> e2 = cadd<T>(a, cconj<T>(b));
+        const C2<T> o2c = cmul<T>(cconj<T>(wk), csub<T>(a, cconj<T>(b)));
+        o1 = cconj<T>(cadd<T>(e2, cmul_i<T>(o2c)));
+        o2 = cconj<T>(cadd<T>(cconj<T>(e2), cmul_i<T>(cconj<T>(o2c))));
+    };
+
+    // Iteration k finishes bin k with its partner: lane ^ 16's v[15 - k]
+    // (warps 1-7), own v[15 - k] (slot 8), own v[(16 - k) mod 16] (slot 0).
+    // Warps 1-7 touch only v[0..7] here, so the partner's shuffles of v[8..15]
+    // always see the forward values.
+    C2<T> send[R / 2];
+#pragma unroll
+    for (int k = 0; k < R / 2; ++k) {
+        C2<T> q;
+        q.x = __shfl_xor_sync(0xffffffffu, v[R - 1 - k].x, 16);
+        q.y = __shfl_xor_sync(0xffffffffu, v[R - 1 - k].y, 16);
+        const int i2 = (slot == 0) ? ((R - k) & (R - 1)) : (R - 1 - k);   // own partner index (warp 0)
+        const C2<T> own = (slot == 0) ? v[(R - k) & (R - 1)] : v[R - 1 - k];
+        C2<T> o1, o2;
+        pair(slot + R * k, v[k], partner_in_warp ? q : own, o1, o2);
+        v[k] = o1;
+        send[k] = o2;
+        if (!partner_in_warp && k > 0) {
+            // warp 0: the partner bin is this thread's own (index i2 > k)
+#pragma unroll
+            for (int j = R / 2; j < R; ++j)
+                if (j == i2) v[j] = o2;
+        } else if (!partner_in_warp && slot == 8) {
+            v[R - 1] = o2;   // k = 0 of slot 8: partner index 15
+        }
+    }
+    if (slot == 0) {   // bin 128 pairs with itself
+        C2<T> o1, o2;
+        pair(R / 2 * R, v[R / 2], v[R / 2], o1, o2);
+        v[R / 2] = o1;
+    }
+    // hand each partner its bins: my send[k] is the partner's v[15 - k]
+#pragma unroll
+    for (int k = 0; k < R / 2; ++k) {
+        C2<T> r;
+        r.x = __shfl_xor_sync(0xffffffffu, send[k].x, 16);
+        r.y = __shfl_xor_sync(0xffffffffu, send[k].y, 16);
+        if (partner_in_warp) v[R - 1 - k] = r;
+    }
+
+    // inverse: stage 0, exchange, stage 1, real outputs x[2m] = Re, x[2m+1] = -Im
+    fast::stage_compute<T, M, 0>(v, slot, tb.twM);
+#pragma unroll
+    for (int k = 0; k < R; ++k) Z[CF::zi(B0::out_idx(slot, 0, k), c)] = v[k];
+    CF::sync();
+#pragma unroll
+    for (int k = 0; k < R; ++k) v[k] = Z[CF::zi(B1::in_idx(slot, 0, k), c)];
+    CF::sync();
+    fast::stage_compute<T, M, 1>(v, slot, tb.twM);
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const int m = slot + R * k;
+        buf[(2 * m) * PR + c] = v[k].x;
+        buf[(2 * m + 1) * PR + c] = -v[k].y;
+    }
 }
 
 // Shared-memory carve-up (byte offsets).
@@ -243,8 +370,9 @@ tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUte
     }
 
     // ---------------- compute ----------------
+    constexpr bool REGSPEC = RegSpectrum<T, M, W, KIND, KIND2>::value;
     const int c = t % W;
-    const int slot = t / W;
+    const int slot = REGSPEC ? paired_slot(t) : t / W;
     for (int i = 0; i < nloc; ++i) {
         const int s = i % kStages;
         if (!mbar_wait(full + s, (uint32_t)((i / kStages) & 1), abort)) {
@@ -265,11 +393,15 @@ tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUte
             s1.dlo = a.dv.lo;
             s1.dhi = a.dv.hi;
             s1.zmax = (a.dv.perturb && col <= a.dv.xz_hi && v <= a.dv.yz_hi) ? a.dv.zz_hi : -1;
-            transform_lines<T, CF, KIND>(buf, red, c, slot, tb, s1);
-            OutSink<T, PR, false> s2;
-            s2.Rv = buf;
-            s2.c = c;
-            transform_lines<T, CF, KIND2>(buf, red, c, slot, tb, s2);
+            if constexpr (REGSPEC) {
+                r2c_div_c2r_regs<T, CF>(buf, c, slot, (t >> 5) != 0, tb, s1);
+            } else {
+                transform_lines<T, CF, KIND>(buf, red, c, slot, tb, s1);
+                OutSink<T, PR, false> s2;
+                s2.Rv = buf;
+                s2.c = c;
+                transform_lines<T, CF, KIND2>(buf, red, c, slot, tb, s2);
+            }
         } else {
             OutSink<T, PR, false> sk;
             sk.Rv = buf;
