@@ -118,30 +118,34 @@ __device__ __forceinline__ void tma_store(const CUtensorMap* map, int c0, int c1
                  : "memory");
 }
 
-// The fused forward / division / inverse pass of N = 512 lines (M = 256, two
-// radix-16 stages) with the spectrum kept in registers.  After the forward
-// stages thread `slot` holds bins m = slot + 16 k; the split, the division and
-// the inverse's pre step need each bin with its partner M - m, held by slot
-// 16 - slot.  Slots are paired in warps (paired_slot): warp w >= 1 holds w
-// and 16 - w, warp 0 the self-paired 0 and 8.  Each pair (m, M - m) is
-// finished once: a thread of warps 1-7 takes the partner's bin of its k < 8 by
-// shuffle, produces the inverse inputs of both bins, keeps its own and hands
-// the partner its, so the spectrum never returns to shared memory.
+// The fused forward / division / inverse pass of N = 512 and N = 256 lines
+// (M = 256: radix 16 x 16; M = 128: radix 16 x 8) with the spectrum kept in
+// registers.  With P = M / 16 threads a line, after the forward stages thread
+// `slot` holds bins m = slot + P k (k = 0..15) -- for M = 128 the last stage
+// takes butterflies slot and slot + 8 to make it so -- which are exactly the
+// inverse's first-stage inputs.  The split, the division and the inverse's
+// pre step need each bin with its partner M - m, held by slot P - slot.  Slots
+// are paired in warps (paired_slot): warp w >= 1 holds w and P - w, warp 0
+// the self-paired 0 and P / 2.  Each pair (m, M - m) is finished once: a thread
+// of warps 1.. takes the partner's bin of its k < 8 by shuffle, produces the
+// inverse inputs of both bins, keeps its own and hands the partner its, so
+// the spectrum never returns to shared memory.
 template <typename T, int M, int WT, int KIND, int KIND2>
 struct RegSpectrum {
-    static constexpr bool value = M == 256 && WT == 16 && KIND == kR2C && KIND2 == kC2R;
+    static constexpr bool value = (M == 256 || M == 128) && WT == 16 && KIND == kR2C && KIND2 == kC2R;
 };
 
+template <int P>
 __device__ __forceinline__ int paired_slot(int t) {
     const int w = t >> 5, h = (t >> 4) & 1;
-    return w == 0 ? 8 * h : (h ? 16 - w : w);
+    return w == 0 ? (P / 2) * h : (h ? P - w : w);
 }
 
 template <typename T, typename CF, typename DSINK>
 __device__ __forceinline__ void r2c_div_c2r_regs(T* buf, int c, int slot, bool partner_in_warp,
                                                  const LineTables<T>& tb, const DSINK& dv) {
-    constexpr int M = CF::M, N = CF::N, PR = CF::PR;
-    static_assert(M == 256 && CF::W == 16 && CF::P == 16, "M = 256, 16-line tiles");
+    constexpr int M = CF::M, N = CF::N, PR = CF::PR, P = CF::P;
+    static_assert((M == 256 || M == 128) && CF::W == 16, "M = 256 or 128, 16-line tiles");
     using B0 = fast::Bfly<M, 0>;
     using B1 = fast::Bfly<M, 1>;
     constexpr int R = fast::kR;
@@ -157,10 +161,34 @@ __device__ __forceinline__ void r2c_div_c2r_regs(T* buf, int c, int slot, bool p
 #pragma unroll
     for (int k = 0; k < R; ++k) Z[CF::zi(B0::out_idx(slot, 0, k), c)] = v[k];
     CF::sync();
+    // u[k] = Z[slot + P k] after the last forward stage
+    C2<T> u[R];
+    if constexpr (M == 256) {
 #pragma unroll
-    for (int k = 0; k < R; ++k) v[k] = Z[CF::zi(B1::in_idx(slot, 0, k), c)];
-    CF::sync();
-    fast::stage_compute<T, M, 1>(v, slot, tb.twM);
+        for (int k = 0; k < R; ++k) v[k] = Z[CF::zi(B1::in_idx(slot, 0, k), c)];
+        CF::sync();
+        fast::stage_compute<T, M, 1>(v, slot, tb.twM);
+#pragma unroll
+        for (int k = 0; k < R; ++k) u[k] = v[k];
+    } else {
+        // radix 8 (Ns = 16, nb = 16) on butterflies j = slot + 8 b: inputs
+        // j + 16 k, twiddles w^(j k), outputs j + 16 k = slot + 8 (b + 2 k)
+        static_assert(B1::r == 8 && B1::Ns == 16 && B1::nb == 16, "M = 128: last stage radix 8");
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[b * 8 + k] = Z[CF::zi(slot + 8 * b + 16 * k, c)];
+        CF::sync();
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const int j = slot + 8 * b;
+#pragma unroll
+            for (int k = 1; k < 8; ++k) v[b * 8 + k] = cmul<T>(v[b * 8 + k], ldtw<T>(tb.twM + j * k));
+            fast::dft_r<T, 8>(v + b * 8);
+        }
+#pragma unroll
+        for (int k = 0; k < R; ++k) u[k] = v[(k & 1) * 8 + (k >> 1)];
+    }
 
     // Pair (m, M - m) from Z[m] = zk, Z[M - m] = zm: the R2C split gives X[m]
     // and X[M - m] (w^(M-m) = -conj w^m), each is divided by its eigenvalue,
@@ -186,60 +214,65 @@ __device__ __forceinline__ void r2c_div_c2r_regs(T* buf, int c, int slot, bool p
         o2 = cconj<T>(cadd<T>(cconj<T>(e2), cmul_i<T>(cconj<T>(o2c))));
     };
 
-    // Iteration k finishes bin k with its partner: lane ^ 16's v[15 - k]
-    // (warps 1-7), own v[15 - k] (slot 8), own v[(16 - k) mod 16] (slot 0).
-    // Warps 1-7 touch only v[0..7] here, so the partner's shuffles of v[8..15]
+    // Iteration k finishes bin k with its partner: lane ^ 16's u[15 - k]
+    // (warps 1..), own u[15 - k] (slot P / 2), own u[(16 - k) mod 16] (slot 0).
+    // Warps 1.. touch only u[0..7] here, so the partner's shuffles of u[8..15]
     // always see the forward values.
     C2<T> send[R / 2];
 #pragma unroll
     for (int k = 0; k < R / 2; ++k) {
         C2<T> q;
-        q.x = __shfl_xor_sync(0xffffffffu, v[R - 1 - k].x, 16);
-        q.y = __shfl_xor_sync(0xffffffffu, v[R - 1 - k].y, 16);
+        q.x = __shfl_xor_sync(0xffffffffu, u[R - 1 - k].x, 16);
+        q.y = __shfl_xor_sync(0xffffffffu, u[R - 1 - k].y, 16);
         const int i2 = (slot == 0) ? ((R - k) & (R - 1)) : (R - 1 - k);   // own partner index (warp 0)
-        const C2<T> own = (slot == 0) ? v[(R - k) & (R - 1)] : v[R - 1 - k];
+        const C2<T> own = (slot == 0) ? u[(R - k) & (R - 1)] : u[R - 1 - k];
         C2<T> o1, o2;
-        pair(slot + R * k, v[k], partner_in_warp ? q : own, o1, o2);
-        v[k] = o1;
+        pair(slot + P * k, u[k], partner_in_warp ? q : own, o1, o2);
+        u[k] = o1;
         send[k] = o2;
         if (!partner_in_warp && k > 0) {
             // warp 0: the partner bin is this thread's own (index i2 > k)
 #pragma unroll
             for (int j = R / 2; j < R; ++j)
-                if (j == i2) v[j] = o2;
-        } else if (!partner_in_warp && slot == 8) {
-            v[R - 1] = o2;   // k = 0 of slot 8: partner index 15
+                if (j == i2) u[j] = o2;
+        } else if (!partner_in_warp && slot == P / 2) {
+            u[R - 1] = o2;   // k = 0 of slot P / 2: partner index 15
         }
     }
-    if (slot == 0) {   // bin 128 pairs with itself
+    if (slot == 0) {   // bin M / 2 pairs with itself
         C2<T> o1, o2;
-        pair(R / 2 * R, v[R / 2], v[R / 2], o1, o2);
-        v[R / 2] = o1;
+        pair(M / 2, u[R / 2], u[R / 2], o1, o2);
+        u[R / 2] = o1;
     }
-    // hand each partner its bins: my send[k] is the partner's v[15 - k]
+    // hand each partner its bins: my send[k] is the partner's u[15 - k]
 #pragma unroll
     for (int k = 0; k < R / 2; ++k) {
         C2<T> r;
         r.x = __shfl_xor_sync(0xffffffffu, send[k].x, 16);
         r.y = __shfl_xor_sync(0xffffffffu, send[k].y, 16);
-        if (partner_in_warp) v[R - 1 - k] = r;
+        if (partner_in_warp) u[R - 1 - k] = r;
     }
 
-    // inverse: stage 0, exchange, stage 1, real outputs x[2m] = Re, x[2m+1] = -Im
-    fast::stage_compute<T, M, 0>(v, slot, tb.twM);
+    // inverse: stage 0 (inputs slot + P k = u[k]), exchange, stage 1, real
+    // outputs x[2m] = Re, x[2m+1] = -Im
+    fast::stage_compute<T, M, 0>(u, slot, tb.twM);
 #pragma unroll
-    for (int k = 0; k < R; ++k) Z[CF::zi(B0::out_idx(slot, 0, k), c)] = v[k];
+    for (int k = 0; k < R; ++k) Z[CF::zi(B0::out_idx(slot, 0, k), c)] = u[k];
     CF::sync();
 #pragma unroll
-    for (int k = 0; k < R; ++k) v[k] = Z[CF::zi(B1::in_idx(slot, 0, k), c)];
-    CF::sync();
-    fast::stage_compute<T, M, 1>(v, slot, tb.twM);
+    for (int b = 0; b < B1::B; ++b)
 #pragma unroll
-    for (int k = 0; k < R; ++k) {
-        const int m = slot + R * k;
-        buf[(2 * m) * PR + c] = v[k].x;
-        buf[(2 * m + 1) * PR + c] = -v[k].y;
-    }
+        for (int k = 0; k < B1::r; ++k) u[b * B1::r + k] = Z[CF::zi(B1::in_idx(slot, b, k), c)];
+    CF::sync();
+    fast::stage_compute<T, M, 1>(u, slot, tb.twM);
+#pragma unroll
+    for (int b = 0; b < B1::B; ++b)
+#pragma unroll
+        for (int k = 0; k < B1::r; ++k) {
+            const int m = B1::out_idx(slot, b, k);
+            buf[(2 * m) * PR + c] = u[b * B1::r + k].x;
+            buf[(2 * m + 1) * PR + c] = -u[b * B1::r + k].y;
+        }
 }
 
 // Shared-memory carve-up (byte offsets).
@@ -372,7 +405,7 @@ tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUte
     // ---------------- compute ----------------
     constexpr bool REGSPEC = RegSpectrum<T, M, W, KIND, KIND2>::value;
     const int c = t % W;
-    const int slot = REGSPEC ? paired_slot(t) : t / W;
+    const int slot = REGSPEC ? paired_slot<CF::P>(t) : t / W;
     for (int i = 0; i < nloc; ++i) {
         const int s = i % kStages;
         if (!mbar_wait(full + s, (uint32_t)((i / kStages) & 1), abort)) {

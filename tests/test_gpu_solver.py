@@ -161,10 +161,15 @@ def test_bad_boundary_code_raises():
     ((24, 40, 512), (0, 0, 0), 0.0),     # singular: zero mode removed in the z pass
     ((36, 20, 512), (3, 3, 0), 0.0),
     ((16, 16, 512), (4, 1, 0), -7.0),
+    ((16, 24, 256), (3, 4, 0), -1.0),
+    ((18, 10, 256), (1, 2, 0), -2.5),
+    ((24, 40, 256), (0, 0, 0), 0.0),     # singular
+    ((36, 20, 256), (3, 3, 0), 0.0),
 ])
 def test_periodic_z_512_vs_oracle(dims, bcs, lam):
-    """Periodic z with N = 512: the fused forward / division / inverse z pass
-    of the TMA kernel on 16-line tiles, the singular cases included."""
+    """Periodic z with N = 512 and 256: the fused forward / division / inverse
+    z pass of the TMA kernel on 16-line tiles with the spectrum held in
+    registers between the transforms, the singular cases included."""
     p = gen.random_problem(*dims, *bcs, lam, seed=7 + sum(bcs))
     assert rel(gpu_solve(p), emulated(p)) < TOL
 
