@@ -45,6 +45,19 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def source_digest() -> str:
+    """SHA-256 (first 16 hex digits) over the library's CUDA sources and
+    headers, by file name: identifies the build a profile was captured on."""
+    import hashlib
+    h = hashlib.sha256()
+    deps = sorted(sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")))
+    for d in deps:
+        h.update(os.path.basename(d).encode())
+        with open(d, "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
 def _compile(src: str, obj: str) -> str:
     cmd = [nvcc_path(), *ARCH_FLAGS, *NVCC_FLAGS, "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC,
            "-c", "-o", obj, src]

@@ -53,13 +53,18 @@ class HostPipeline:
         return n + faces, n
 
     def solve(self, f_hosts: Sequence[torch.Tensor], u_hosts: Sequence[torch.Tensor]) -> None:
-        """u_hosts[i] <- solution for f_hosts[i] (host tensors; pinned for the
-        copies to overlap).  Returns once every copy is queued; call
-        ``join()`` and synchronise that stream before reading u_hosts."""
+        """u_hosts[i] <- solution for f_hosts[i] (contiguous host tensors; pinned
+        for the copies to overlap, otherwise each copy blocks the host).
+        Returns once every copy is queued; call ``join()`` and synchronise that
+        stream before reading u_hosts.  Raises ValueError for a non-contiguous
+        tensor (a reshaped copy would silently drop the result)."""
         nx, ny, nz = self.dims
         xbc, ybc, zbc = self.bcs
         d = self.dom
         k = len(self.slots)
+        for t in list(f_hosts) + list(u_hosts):
+            if not t.is_contiguous():
+                raise ValueError("HostPipeline.solve needs contiguous host tensors")
         for i, (fh, uh) in enumerate(zip(f_hosts, u_hosts)):
             s = i % k
             f = self.slots[s]
@@ -67,10 +72,10 @@ class HostPipeline:
             with torch.cuda.stream(self.s_in):
                 if self.used[s]:
                     self.s_in.wait_event(self.ev_out[s])   # the slot's previous result is out
-                f.copy_(fh.reshape(-1), non_blocking=True)
+                f.copy_(fh.view(-1), non_blocking=True)
                 for key, v in self.faces_h.items():
                     if v is not None:
-                        fc[key].copy_(v.reshape(-1), non_blocking=True)
+                        fc[key].copy_(v.contiguous().view(-1), non_blocking=True)
                 self.ev_in[s].record(self.s_in)
             with torch.cuda.stream(self.s_run):
                 self.s_run.wait_event(self.ev_in[s])
@@ -81,7 +86,7 @@ class HostPipeline:
                 self.ev_run[s].record(self.s_run)
             with torch.cuda.stream(self.s_out):
                 self.s_out.wait_event(self.ev_run[s])
-                uh.reshape(-1).copy_(f, non_blocking=True)
+                uh.view(-1).copy_(f, non_blocking=True)
                 self.ev_out[s].record(self.s_out)
             self.used[s] = True
 

@@ -1,9 +1,12 @@
 /* Drop-in replacement for the reference's cudasymmfft/global.h: the transform
  * kind enum with the same enumerators and values (global.h:6-15), which are
- * part of the do_transform ABI.  The reference's cuFFT error-string table is
- * not needed: no cuFFT is used. */
+ * part of the do_transform ABI, and the TRANS_BLOCK_DIM macro (global.h:5) for
+ * callers that size their own blocks with it.  The reference's cuFFT
+ * error-string table is not needed: no cuFFT is used. */
 #ifndef __GLOBAL__
 #define __GLOBAL__
+
+#define TRANS_BLOCK_DIM 16
 
 enum transform_kind {
     DCT_1,
