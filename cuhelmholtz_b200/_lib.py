@@ -72,6 +72,9 @@ SIGNATURES = {
     "chz_launch_count": (ctypes.c_ulonglong, []),
     "chz_set_kernel_family": (c_int, [c_int]),
     "chz_debug_flags": (c_int, [c_int]),
+    "chz_stream_status": (c_int, [c_void_p]),
+    "chz_set_wait_limit": (ctypes.c_longlong, [ctypes.c_longlong]),
+    "chz_wait_selftest": (c_int, [ctypes.c_longlong, c_void_p]),
 }
 
 

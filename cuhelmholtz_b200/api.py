@@ -16,6 +16,7 @@ stream-ordered on torch's current stream; they do not synchronise.
 """
 from __future__ import annotations
 
+import ctypes
 from typing import Optional
 
 import torch
@@ -33,6 +34,7 @@ CHZ_ERROR_NOT_CUBIC = 3
 CHZ_ERROR_CUDA = 4
 CHZ_ERROR_ALLOC = 5
 CHZ_ERROR_WORKSPACE = 6
+CHZ_ERROR_TIMEOUT = 7
 
 
 class CHZError(RuntimeError):
@@ -279,6 +281,27 @@ def set_kernel_family(family) -> int:
 def debug_flags(reset: bool = True) -> int:
     """Flags raised by the kernels' bounded waits (0: none ran out)."""
     return int(_lib.lib().chz_debug_flags(1 if reset else 0))
+
+
+def stream_status(stream=None) -> None:
+    """Waits for ``stream`` (default: the current one) and raises CHZError
+    (CHZ_ERROR_TIMEOUT) when a kernel of this library gave up one of its
+    bounded waits since the last check -- the results queued since then are
+    not valid -- or CHZ_ERROR_CUDA on a CUDA error."""
+    _check(_lib.lib().chz_stream_status(ctypes.c_void_p(_stream(stream))))
+
+
+def set_wait_limit(cycles: int) -> int:
+    """Limit of the kernels' bounded waits in SM clock cycles (>= 1e6; <= 0
+    restores the default of 2e9).  Returns the previous limit."""
+    return int(_lib.lib().chz_set_wait_limit(int(cycles)))
+
+
+def wait_selftest(cycles: int = 1_000_000, stream=None) -> None:
+    """Queues the self-test kernel whose wait runs out after ``cycles`` SM
+    clock cycles (nothing arrives at its barrier); ``stream_status`` then
+    raises CHZ_ERROR_TIMEOUT."""
+    _check(_lib.lib().chz_wait_selftest(int(cycles), ctypes.c_void_p(_stream(stream))))
 
 
 def workspace_size(NX: int, NY: int, NZ: int, precision: int = 0) -> int:

@@ -516,6 +516,7 @@ const char* chz_status_string(int status) {
         case CHZ_ERROR_CUDA: return "CHZ_ERROR_CUDA";
         case CHZ_ERROR_ALLOC: return "CHZ_ERROR_ALLOC";
         case CHZ_ERROR_WORKSPACE: return "CHZ_ERROR_WORKSPACE";
+        case CHZ_ERROR_TIMEOUT: return "CHZ_ERROR_TIMEOUT";
         default: return "CHZ_ERROR_UNKNOWN";
     }
 }
@@ -614,6 +615,23 @@ static void exit_on(int rc, int code) {
     exit(code);
 }
 
+// After the synchronous entry points' device synchronisation: a CUDA error,
+// or a kernel wait that ran out (its results are not valid), ends the process
+// as the reference's CUDA error checks do (funcinterface.cu:104-107,
+// cuda_helmholtz_solver.cu:22-29).
+static void exit_on_device_error(int code) {
+    const cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        printf("CUDA ERROR: %s !\n", cudaGetErrorString(e));
+        exit(code);
+    }
+    const int flags = chz_debug_flags(1);
+    if (flags != 0) {
+        printf("cuhelmholtz_b200: a kernel wait ran out (flags %d)\n", flags);
+        exit(code);
+    }
+}
+
 // funcinterface.cu:25-40
 void do_transform(double* d_data, double* d_out, int NX, int NY, int NZ, transform_kind X_TRANS,
                   transform_kind Y_TRANS, transform_kind Z_TRANS) {
@@ -623,33 +641,21 @@ void do_transform(double* d_data, double* d_out, int NX, int NY, int NZ, transfo
         exit(0);
     }
     exit_on(rc, 0);
-    const cudaError_t e = cudaDeviceSynchronize();
-    if (e != cudaSuccess) {
-        printf("CUDA ERROR: %s !\n", cudaGetErrorString(e));
-        exit(0);
-    }
+    exit_on_device_error(0);
 }
 
 // funcinterface.cu:200-334
 void do_transform_nocubic(double* d_data, double* d_out, int NX, int NY, int NZ, transform_kind X_TRANS,
                           transform_kind Y_TRANS, transform_kind Z_TRANS) {
     exit_on(chz_do_transform_any(d_data, d_out, NX, NY, NZ, X_TRANS, Y_TRANS, Z_TRANS, nullptr), 0);
-    const cudaError_t e = cudaDeviceSynchronize();
-    if (e != cudaSuccess) {
-        printf("CUDA ERROR: %s !\n", cudaGetErrorString(e));
-        exit(0);
-    }
+    exit_on_device_error(0);
 }
 
 // funcinterface.cu:42-198
 void do_transform_cubic(double* d_data, int NX, int NY, int NZ, transform_kind X_TRANS,
                         transform_kind Y_TRANS, transform_kind Z_TRANS) {
     exit_on(chz_do_transform_any(d_data, d_data, NX, NY, NZ, X_TRANS, Y_TRANS, Z_TRANS, nullptr), 0);
-    const cudaError_t e = cudaDeviceSynchronize();
-    if (e != cudaSuccess) {
-        printf("CUDA ERROR: %s !\n", cudaGetErrorString(e));
-        exit(0);
-    }
+    exit_on_device_error(0);
 }
 
 // funcinterface.cu:337-342
@@ -669,10 +675,6 @@ int cuda_helmholtz_solver(double left, double right, int NX, int xbc, double* bc
         std::printf("%s\n", chz_last_error());
         exit(-1);
     }
-    const cudaError_t e = cudaDeviceSynchronize();
-    if (e != cudaSuccess) {
-        std::printf("%s\n", cudaGetErrorString(e));
-        exit(-1);
-    }
+    exit_on_device_error(-1);
     return 0;
 }

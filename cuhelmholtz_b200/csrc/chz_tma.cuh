@@ -19,8 +19,11 @@
 // keeps the spectrum in registers between the two transforms
 // (r2c_div_c2r_regs).
 //
-// Waits are bounded: a wait that runs out sets a flag that the host can read
-// (chz_debug_flags) and the thread carries on, so the kernel always ends.
+// Waits are bounded: a wait that runs out sets a flag that the host reads
+// (chz_stream_status, chz_debug_flags) and the thread carries on, so the
+// kernel always ends; before it ends the producer waits (bounded as well) for
+// the last load of every stage, so no copy into the CTA's shared memory is in
+// flight when it exits.
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -82,24 +85,60 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* b) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(saddr(b)) : "memory");
 }
 
+__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
 // Waits for the phase with the given parity to complete.  Gives up after
-// about a second of SM clock, or at once when another thread of the CTA has
-// given up (*abort), so a CTA whose copies never arrive still ends quickly.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort) {
+// `limit` SM clock cycles (the host sets it: about a second by default), or
+// at once when another thread of the CTA has given up (*abort), so a CTA
+// whose copies never arrive still ends quickly.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort, long long limit) {
     const uint32_t a = saddr(b);
     const long long t0 = clock64();
     while (true) {
-        uint32_t ok;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(ok)
-            : "r"(a), "r"(parity)
-            : "memory");
-        if (ok) return true;
-        if (*abort || clock64() - t0 > 2000000000LL) {
+        if (mbar_try(a, parity)) return true;
+        if (*abort || clock64() - t0 > limit) {
             *abort = 1;
             return false;
         }
+    }
+}
+
+// The producer's last wait before the CTA ends: the phase of the last load
+// issued into a stage, waited for whether or not the CTA has given up, so no
+// copy into this CTA's shared memory is still in flight when it exits (after
+// a normal run the phase is already complete).  Bounded by `limit` too.
+__device__ __forceinline__ bool mbar_drain(uint64_t* b, uint32_t parity, long long limit) {
+    const uint32_t a = saddr(b);
+    const long long t0 = clock64();
+    while (!mbar_try(a, parity)) {
+        if (clock64() - t0 > limit) return false;
+    }
+    return true;
+}
+
+// Bit of the device flag word each kind of wait raises when it runs out.
+enum WaitFlag {
+    kFlagProducer = 1,    // the producer gave up waiting for a finished tile
+    kFlagConsumer = 2,    // a compute thread gave up waiting for a tile load
+    kFlagAlign = 4,       // misaligned shared memory (nothing was started)
+    kFlagDrain = 8,       // a load was still in flight when the CTA ended
+    kFlagSelfTest = 16    // the wait of chz_wait_selftest ran out (as it should)
+};
+
+// The producer's drain: for every stage that received loads, the phase of
+// the last load issued into it (tile i of this CTA loads stage i % kStages).
+__device__ __forceinline__ void drain_loads(uint64_t* full, int nloc, int stages, long long limit, int* flags) {
+    for (int s = 0; s < stages && s < nloc; ++s) {
+        const int last = s + ((nloc - 1 - s) / stages) * stages;
+        if (!mbar_drain(full + s, (uint32_t)((last / stages) & 1), limit)) atomicOr(flags, kFlagDrain);
     }
 }
 
@@ -301,7 +340,7 @@ struct TmaSmem {
 template <typename T, int M, int KIND, int KIND2>
 __global__ void __launch_bounds__(TCfg<T, M>::NT + 32, 1)
 tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUtensorMap stmap, PassArgs a,
-         LineTables<T> tg, TmaGeom g, int ntx, int ntiles, int* flags) {
+         LineTables<T> tg, TmaGeom g, int ntx, int ntiles, int* flags, long long wait_limit) {
     using CF = TCfg<T, M>;
     constexpr bool DCTTAB = UsesDctTables<KIND, KIND2>::value;
     using SL = TmaSmem<T, M, (KIND2 >= 0), DCTTAB>;
@@ -310,7 +349,7 @@ tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUte
     const int t = threadIdx.x;
     if ((int)blockIdx.x >= ntiles) return;
     if (saddr(smem_raw) & 127) {  // uniform over the CTA: nothing has started
-        if (t == 0) atomicOr(flags, 4);
+        if (t == 0) atomicOr(flags, kFlagAlign);
         return;
     }
     const int rb = g.rows_buf;
@@ -380,7 +419,8 @@ tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUte
         for (int i = 0; i < pre; ++i) issue_load(i);
         for (int i = 0; i < nloc; ++i) {
             const int s = i % kStages;
-            if (!mbar_wait(ready + s, (uint32_t)((i / kStages) & 1), abort)) atomicOr(flags, 1);
+            if (!mbar_wait(ready + s, (uint32_t)((i / kStages) & 1), abort, wait_limit))
+                atomicOr(flags, kFlagProducer);
             const int tile = (int)blockIdx.x + i * (int)gridDim.x;
             const int cx = (tile % ntx) * W;
             const int v = a.v0 + tile / ntx;
@@ -399,6 +439,7 @@ tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUte
             }
         }
         asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+        drain_loads(full, nloc, kStages, wait_limit, flags);
         return;
     }
 
@@ -408,8 +449,8 @@ tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUte
     const int slot = REGSPEC ? paired_slot<CF::P>(t) : t / W;
     for (int i = 0; i < nloc; ++i) {
         const int s = i % kStages;
-        if (!mbar_wait(full + s, (uint32_t)((i / kStages) & 1), abort)) {
-            if (t == 0) atomicOr(flags, 2);
+        if (!mbar_wait(full + s, (uint32_t)((i / kStages) & 1), abort, wait_limit)) {
+            if (t == 0) atomicOr(flags, kFlagConsumer);
         }
         T* buf = reinterpret_cast<T*>(smem_raw + (size_t)s * sbytes);
         const int tile = (int)blockIdx.x + i * (int)gridDim.x;

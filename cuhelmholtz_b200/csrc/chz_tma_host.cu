@@ -1,6 +1,8 @@
 // Host support of the TMA-pipelined pass: tensor-map encoding through the
 // driver entry point (no link against the driver library), the device flag
-// word of the kernels' bounded waits, and the shared-memory limit.
+// word and the limit of the kernels' bounded waits, the status check that
+// reads the flag word, a self-test of a wait that runs out, and the
+// shared-memory limit.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -8,6 +10,7 @@
 #include <mutex>
 
 #include "chz_internal.h"
+#include "chz_tma.cuh"
 #include "cuhelmholtz_b200.h"
 
 namespace chz {
@@ -31,10 +34,35 @@ EncodeTiledFn encoder() {
     return fn;
 }
 
-// Bit 0: the producer gave up waiting for a finished tile; bit 1: a compute
-// thread gave up waiting for a tile load; bit 2: misaligned shared memory.
+// Bits of WaitFlag (chz_tma.cuh) raised by the waits that ran out.
 __device__ int g_flags;
+
+// Limit of every bounded wait of the pipelined kernels, in SM clock cycles
+// (about a second at the B200's clocks by default).
+constexpr long long kDefaultWaitLimit = 2000000000LL;
+constexpr long long kMinWaitLimit = 1000000LL;
+std::atomic<long long> g_wait_limit{kDefaultWaitLimit};
+
+// One CTA that waits on an mbarrier nothing ever arrives at: the wait must
+// run out after `limit` cycles and raise kFlagSelfTest.  No copy is issued,
+// so nothing is in flight when the CTA ends.
+__global__ void wait_selftest_kernel(int* flags, long long limit) {
+    __shared__ uint64_t bar;
+    __shared__ int abort;
+    if (threadIdx.x == 0) {
+        abort = 0;
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    if (!mbar_wait(&bar, 0u, &abort, limit)) {
+        if (threadIdx.x == 0) atomicOr(flags, kFlagSelfTest);
+    }
+    __syncthreads();
+}
 }  // namespace
+
+long long wait_limit() { return g_wait_limit.load(std::memory_order_relaxed); }
 
 bool encode_map(CUtensorMap* map, bool is_double, const void* base, const unsigned long long dims[3],
                 const unsigned long long strides[2], const unsigned box[3]) {
@@ -114,4 +142,35 @@ extern "C" int chz_debug_flags(int reset) {
         if (cudaMemcpy(p, &z, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) return -1;
     }
     return v;
+}
+
+extern "C" long long chz_set_wait_limit(long long cycles) {
+    using namespace chz::tma;
+    if (cycles <= 0) cycles = kDefaultWaitLimit;
+    if (cycles < kMinWaitLimit) cycles = kMinWaitLimit;
+    return g_wait_limit.exchange(cycles);
+}
+
+extern "C" int chz_stream_status(void* stream) {
+    const cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return chz::cuda_fail((int)e, "chz_stream_status");
+    const int v = chz_debug_flags(1);
+    if (v < 0) return chz::cuda_fail((int)cudaGetLastError(), "chz_stream_status: reading the wait flags");
+    if (v != 0)
+        return chz::fail(CHZ_ERROR_TIMEOUT,
+                         "a kernel wait ran out (flags 0x%x): the results of the work queued since the last "
+                         "status check are not valid",
+                         v);
+    return CHZ_SUCCESS;
+}
+
+extern "C" int chz_wait_selftest(long long cycles, void* stream) {
+    int* flags = chz::tma::device_flags();
+    if (!flags) return chz::cuda_fail((int)cudaGetLastError(), "chz_wait_selftest");
+    if (cycles < 1000) cycles = 1000;
+    if (cycles > chz::tma::kDefaultWaitLimit) cycles = chz::tma::kDefaultWaitLimit;
+    chz::tma::wait_selftest_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(flags, cycles);
+    chz::count_launch();
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? CHZ_SUCCESS : chz::cuda_fail((int)e, "chz_wait_selftest");
 }

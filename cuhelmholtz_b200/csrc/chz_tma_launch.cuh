@@ -21,6 +21,8 @@ namespace tma {
 bool encode_map(CUtensorMap* map, bool is_double, const void* base, const unsigned long long dims[3],
                 const unsigned long long strides[2], const unsigned box[3]);
 int* device_flags();
+// limit of the kernels' bounded waits, in SM clock cycles (chz_set_wait_limit)
+long long wait_limit();
 int max_optin_smem();
 
 template <int KIND, int N>
@@ -115,7 +117,7 @@ int launch_one(const T* in, T* out, const PassArgs& a, const LineTables<T>& tb, 
     const long long cap = (long long)cps * fast::device_sm_count();
     const int grid = (int)std::min(ntiles, cap);
     trace_begin(stream, label);
-    kern<<<grid, threads, smem, stream>>>(ldmap, stmap, a, tb, g, ntx, (int)ntiles, flags);
+    kern<<<grid, threads, smem, stream>>>(ldmap, stmap, a, tb, g, ntx, (int)ntiles, flags, wait_limit());
     count_launch();
     trace_end(stream);
     return (int)cudaGetLastError();

@@ -110,7 +110,8 @@ __device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* b) {
 template <typename T, int M, int KIND, bool LD_TMA, bool ST_TMA>
 __global__ void __launch_bounds__(XCfg<M>::NT + 32, 1)
 xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUtensorMap stmap, const T* in,
-          T* out, PassArgs a, LineTables<T> tg, XGeom g, int ntx, int ntiles, int* flags) {
+          T* out, PassArgs a, LineTables<T> tg, XGeom g, int ntx, int ntiles, int* flags,
+          long long wait_limit) {
     using CF = XCfg<M>;
     using SL = XSmem<T, M>;
     constexpr int W = CF::W, NT = CF::NT, N = CF::N;
@@ -196,7 +197,8 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
             for (int i = 0; i < pre; ++i) issue_load(i);
             for (int i = 0; i < nloc; ++i) {
                 const int s = i % kStages;
-                if (!mbar_wait(ready + s, (uint32_t)((i / kStages) & 1), abort)) atomicOr(flags, 1);
+                if (!mbar_wait(ready + s, (uint32_t)((i / kStages) & 1), abort, wait_limit))
+                    atomicOr(flags, tma::kFlagProducer);
                 if constexpr (ST_TMA) {
                     if (lane == 0) {
                         const int tile = (int)blockIdx.x + i * (int)gridDim.x;
@@ -222,6 +224,9 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
                 if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
             }
             if constexpr (!LD_TMA) asm volatile("cp.async.wait_all;\n" ::: "memory");
+            if constexpr (LD_TMA) {
+                if (lane == 0) tma::drain_loads(full, nloc, kStages, wait_limit, flags);
+            }
         }
         return;
     }
@@ -232,8 +237,8 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
     const double sc = a.use_scale ? a.scale : 1.0;
     for (int i = 0; i < nloc; ++i) {
         const int s = i % kStages;
-        if (!mbar_wait(full + s, (uint32_t)((i / kStages) & 1), abort)) {
-            if (t == 0) atomicOr(flags, 2);
+        if (!mbar_wait(full + s, (uint32_t)((i / kStages) & 1), abort, wait_limit)) {
+            if (t == 0) atomicOr(flags, tma::kFlagConsumer);
         }
         T* buf = stage_of(s);
         const int tile = (int)blockIdx.x + i * (int)gridDim.x;

@@ -18,6 +18,7 @@ namespace tma {
 bool encode_map_swz(CUtensorMap* map, const void* base, const unsigned long long dims[3],
                     const unsigned long long strides[2], const unsigned box[3]);
 int* device_flags();
+long long wait_limit();
 int max_optin_smem();
 }  // namespace tma
 namespace xtma {
@@ -79,7 +80,7 @@ int launch_one(const double* in, double* out, const PassArgs& a, const LineTable
     const long long cap = (long long)cps * fast::device_sm_count();
     const int grid = (int)std::min(ntiles, cap);
     trace_begin(stream, label);
-    kern<<<grid, threads, SL::total, stream>>>(ldmap, stmap, in, out, a, tb, g, ntx, (int)ntiles, flags);
+    kern<<<grid, threads, SL::total, stream>>>(ldmap, stmap, in, out, a, tb, g, ntx, (int)ntiles, flags, tma::wait_limit());
     count_launch();
     trace_end(stream);
     return (int)cudaGetLastError();

@@ -35,7 +35,8 @@ typedef enum chz_status {
     CHZ_ERROR_NOT_CUBIC = 3,        /* in-place do_transform on a non-cubic grid */
     CHZ_ERROR_CUDA = 4,             /* a CUDA runtime call failed */
     CHZ_ERROR_ALLOC = 5,            /* device allocation failed */
-    CHZ_ERROR_WORKSPACE = 6         /* caller workspace too small or misaligned */
+    CHZ_ERROR_WORKSPACE = 6,        /* caller workspace too small or misaligned */
+    CHZ_ERROR_TIMEOUT = 7           /* a kernel's bounded wait ran out (see chz_stream_status) */
 } chz_status;
 
 /* transform kinds: same values as the reference's enum transform_kind
@@ -82,8 +83,6 @@ int chz_helmholtz_solve(double left, double right, int nx, int xbc,
                         const double* bcf, const double* bce,
                         double lambda, double* f, void* stream);
 
-/* As chz_helmholtz_solve with a caller-owned device workspace of at least
- * chz_helmholtz_workspace_size(nx, ny, nz, 0) bytes, 256-byte aligned. */
 /* The solve with the reference's 19-point variant (_nonpoisson_devide_19points_,
  * _cuda_helmholtz_.inl:255-274, commented out at cuda_helmholtz_solver.cu:325
  * and :338): the spectral division by the eigenvalues of the compact 19-point
@@ -119,6 +118,8 @@ int chz_helmholtz_solve_pertrb(double left, double right, int nx, int xbc,
                                const double* bcf, const double* bce,
                                double lambda, double* f, double* pertrb, void* stream);
 
+/* As chz_helmholtz_solve with a caller-owned device workspace of at least
+ * chz_helmholtz_workspace_size(nx, ny, nz, 0) bytes, 256-byte aligned. */
 int chz_helmholtz_solve_ws(double left, double right, int nx, int xbc,
                            const double* bcl, const double* bcr,
                            double bottom, double top, int ny, int ybc,
@@ -251,6 +252,32 @@ int chz_set_kernel_family(int family);
 /* Flags raised by the kernels' bounded waits since the last reset (0 when no
  * wait ran out); reset != 0 clears them.  Synchronous.  -1 on a CUDA error. */
 int chz_debug_flags(int reset);
+
+/* Status of the work queued on `stream`: waits for it, then returns
+ * CHZ_ERROR_TIMEOUT (and clears the flags) when a kernel of this library on
+ * the current device gave up one of its bounded waits since the last check --
+ * its results are then not valid -- CHZ_ERROR_CUDA on a CUDA error, else
+ * CHZ_SUCCESS.  The stream-ordered entry points return before their kernels
+ * run, so a wait that runs out surfaces here (the reference's synchronous
+ * C++ entry points in funcinterface.h / cuda_helmholtz_solver.h check it
+ * themselves and exit, as they do on a CUDA error).  No counterpart in the
+ * reference, whose kernels have no waits. */
+int chz_stream_status(void* stream);
+
+/* Limit of the pipelined kernels' bounded waits on a tile copy or a finished
+ * tile, in SM clock cycles (default 2e9, about a second; values below 1e6 are
+ * raised to 1e6, <= 0 restores the default).  A wait that runs out raises a
+ * flag, its CTA stops waiting and ends after its own copies have landed, and
+ * chz_stream_status reports CHZ_ERROR_TIMEOUT.  Applies to launches made
+ * after the call.  Returns the previous limit. */
+long long chz_set_wait_limit(long long cycles);
+
+/* Self-test of the bounded-wait path: one CTA waits `cycles` SM clock cycles
+ * (clamped to 1e3 .. 2e9) on an mbarrier that nothing arrives at, the wait
+ * runs out and raises a flag, and the kernel ends; chz_stream_status(stream)
+ * then returns CHZ_ERROR_TIMEOUT.  No copy is issued and the context stays
+ * usable.  Stream-ordered. */
+int chz_wait_selftest(long long cycles, void* stream);
 
 /* Number of kernel launches this library has issued in this process. */
 unsigned long long chz_launch_count(void);

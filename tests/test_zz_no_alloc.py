@@ -58,6 +58,40 @@ def test_noalloc_matches_allocating_solver_on_two_calls_in_a_row():
         assert rel < TOL, rel
 
 
+@pytest.mark.parametrize("dims,codes", [((48, 40, 512), (3, 4, 0)),    # TMA z pass, spectrum in registers
+                                        ((64, 48, 256), (1, 2, 0))])   # the same at N = 256
+def test_noalloc_tma_z_pass_on_the_static_arrays(dims, codes):
+    """Lengths 256 and 512 on z take the TMA-pipelined z pass, whose tensor
+    maps are then built over the __device__ work array."""
+    L = _lib.lib()
+    p = gen.random_problem(*dims, *codes, -1.0, seed=33)
+    for _ in range(2):
+        a = _solve(L.chz_helmholtz_solve_noalloc, p)
+        b = _solve(L.chz_helmholtz_solve, p)
+        rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+        assert rel < TOL, rel
+
+
+def test_noalloc_allocates_no_device_memory():
+    """With every library cache released, a call of a size the library has
+    just released leaves the device's free memory unchanged (an allocation by
+    the library would take at least one 2 MiB page)."""
+    L = _lib.lib()
+    p = gen.random_problem(72, 56, 80, 0, 3, 2, -2.5, seed=34)
+    _solve(L.chz_helmholtz_solve_noalloc, p)      # loads the kernels this size uses
+    torch.cuda.synchronize()
+    assert L.chz_release_cached() == 0
+    torch.cuda.empty_cache()
+    free0, _ = torch.cuda.mem_get_info()
+    f, faces = _device(p)                          # input and output only (torch allocates them)
+    free1, _ = torch.cuda.mem_get_info()
+    st = L.chz_helmholtz_solve_noalloc(*_args(p, f, faces))
+    assert st == 0, L.chz_last_error()
+    torch.cuda.synchronize()
+    free2, _ = torch.cuda.mem_get_info()
+    assert free2 == free1, (free0, free1, free2)
+
+
 def test_noalloc_rejects_problems_beyond_its_scratch():
     L = _lib.lib()
     p = dict(nx=512, ny=512, nz=512, xbc=1, ybc=1, zbc=1, dom=gen.UNIT_DOMAIN, lam=-1.0)
