@@ -73,6 +73,14 @@ SIGNATURES = {
     "chz_set_kernel_family": (c_int, [c_int]),
     "chz_debug_flags": (c_int, [c_int]),
     "chz_stream_status": (c_int, [c_void_p]),
+    "chz_slab_forward": (c_int, [c_double, c_double, c_int, c_int, _dp, _dp, c_double, c_double, c_int, c_int,
+                                 _dp, _dp, c_double, c_double, c_int, c_int, _dp, _dp, _dp, c_int, c_int, _dp,
+                                 c_void_p]),
+    "chz_slab_z": (c_int, [c_double, c_double, c_int, c_int, c_double, c_double, c_int, c_int, c_double,
+                           c_double, c_int, c_int, c_double, _dp, c_int, c_int, c_void_p]),
+    "chz_slab_inverse": (c_int, [c_double, c_double, c_int, c_int, c_double, c_double, c_int, c_int, c_double,
+                                 c_double, c_int, c_int, _dp, _dp, c_int, c_int, c_void_p]),
+    "chz_slab_work_elems": (c_size_t, [c_int, c_int, c_int]),
     "chz_set_wait_limit": (ctypes.c_longlong, [ctypes.c_longlong]),
     "chz_wait_selftest": (c_int, [ctypes.c_longlong, c_void_p]),
 }

@@ -217,24 +217,27 @@ struct OutSink {
     __device__ static __forceinline__ double recip(double d) { return recip_nr(d); }
 };
 
-// One complete real transform of the W lines held in `buf` (real view in,
-// real view out).
-template <typename T, typename CF, int KIND, typename SINK>
-__device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot, const LineTables<T>& tb,
-                                                const SINK& sink) {
+// One complete real transform of the W lines held in `buf`: the real input of
+// line c is read through the view X (entry l: X(l)), the complex exchange view
+// Z[m * W + c] reuses `buf` once every input is in registers, and the real
+// output goes to `sink`.
+template <typename T, typename CF, int KIND, typename V, typename SINK>
+__device__ __forceinline__ void transform_lines_v(const V& X, T* buf, T* red, int c, int slot,
+                                                  const LineTables<T>& tb, const SINK& sink) {
     constexpr int M = CF::M;
     constexpr int W = CF::W, N = CF::N, P = CF::P;
     constexpr bool FWD = (KIND == kR2C || KIND == kDCT2 || KIND == kDST2);
-    const auto X = CF::reader(static_cast<const T*>(buf), c);
     C2<T>* Z = reinterpret_cast<C2<T>*>(buf);
     C2<T> v[kR];
 
-    // DCT1: partial sums of the odd entries x[1], x[3], ..., x[N-1]
+    // DCT1: partial sums of the odd entries x[1], x[3], ..., x[N-1] -- the
+    // entries x[2n + 1] the pre step reads for this thread's inputs n, so the
+    // partial sum is published only after those reads (no store between them
+    // lets the compiler load each entry once)
+    T acc = T(0);
     if constexpr (KIND == kDCT1) {
-        T acc = T(0);
 #pragma unroll
         for (int q = 0; q < M / P; ++q) acc += X(2 * (slot + q * P) + 1);
-        red[slot * W + c] = acc;
     }
 
     // ---- stage 0: pre step fused into the reads ----
@@ -242,6 +245,7 @@ __device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot,
         using BF = Bfly<M, 0>;
 #pragma unroll
         for (int k = 0; k < kR; ++k) v[k] = pre_value<T, KIND, M>(X, BF::in_idx(slot, 0, k), tb);
+        if constexpr (KIND == kDCT1) red[slot * W + c] = acc;
         CF::sync();
         stage_compute<T, M, 0>(v, slot, tb.twM);
     }
@@ -398,6 +402,13 @@ __device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot,
             }
     }
     CF::sync();
+}
+
+// The same with the configuration's own real view of `buf`.
+template <typename T, typename CF, int KIND, typename SINK>
+__device__ __forceinline__ void transform_lines(T* buf, T* red, int c, int slot, const LineTables<T>& tb,
+                                                const SINK& sink) {
+    transform_lines_v<T, CF, KIND>(CF::reader(static_cast<const T*>(buf), c), buf, red, c, slot, tb, sink);
 }
 
 template <int KIND, int N>

@@ -8,14 +8,19 @@
 // CU_TENSOR_MAP_SWIZZLE_128B lands as.  Entry l of line c is therefore at
 //   (l / 16) * 256 + c * 16 + 2 * (((l / 2) mod 8) ^ (c mod 8)) + (l mod 2).
 // A side of the pass on a 16-byte-aligned array (a padded do_transform array,
-// the solver's work array) moves by tensor copies; a side on an array with
-// 8-byte-aligned rows (the solver's f) is copied by the producer warp with
-// cp.async (32 consecutive entries of a row per instruction, each a whole
-// swizzled row: conflict-free), whose completion the stage's mbarrier tracks
-// (cp.async.mbarrier.arrive.noinc), or stored by the compute warps.  The host
-// takes the kernel only where both sides are tensor copies (the faster case).  The transform is the register-resident
-// radix-16 line transform of chz_fast.cuh on this layout (real-view reads of
-// one entry by the 16 lines of a slot hit each bank pair at most twice).
+// the solver's work array) moves by tensor copies in that layout.  A side on
+// an array whose rows are only 8-byte aligned (the solver's f, rows of N + 1
+// values) moves untiled instead: the W rows of a tile are one contiguous span
+// of memory, so a load is a single cp.async.bulk of the span widened to
+// 16-byte boundaries, landing row-major (entry l of line c at
+// off + c * pitch + l, off = 0 or 1 the span's misalignment), and a store
+// leaves row-major the same way: one cp.async.bulk per row of the 16-byte-
+// aligned interior of its output window (one for the whole tile when the
+// window is whole rows), the 8-byte ends by plain stores, so neighbouring
+// tiles never write the same 16 bytes.  The transform is the
+// register-resident radix-16 line transform of chz_fast.cuh on either layout
+// (swizzled: the 16 lines of a slot hit each bank pair at most twice; row-major
+// with an odd pitch: once).
 #pragma once
 #include "chz_tma.cuh"
 
@@ -24,6 +29,7 @@ namespace xtma {
 
 using fast::OutSink;
 using fast::transform_lines;
+using fast::transform_lines_v;
 using tma::kStages;
 using tma::mbar_arrive;
 using tma::mbar_expect_tx;
@@ -104,10 +110,68 @@ __device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* b) {
     asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(saddr(b)) : "memory");
 }
 
-// LD_TMA: the input moves by tensor loads (ldmap), else the producer warp
-// copies it with cp.async; ST_TMA: the output moves by tensor stores (stmap),
-// else the compute warps store it.
-template <typename T, int M, int KIND, bool LD_TMA, bool ST_TMA>
+// How each side of a tile moves.
+enum XLoad { kLdTensor = 0, kLdSpan = 1 };
+enum XStore { kStTensor = 0, kStRows = 1 };
+
+// Row-major real view of one line (span loads): entry l at line[l].
+template <typename T>
+struct RowView {
+    const T* __restrict__ line;
+    __device__ __forceinline__ T operator()(int l) const { return line[l]; }
+};
+
+// Output sink of the row-major view (row stores), scaled as it is written.
+template <typename T>
+struct RowSink {
+    T* line;
+    double sc;
+    __device__ __forceinline__ void put(int l, T v) const { line[l] = (T)((double)v * sc); }
+    __device__ __forceinline__ void put_pair(int l, T re, T im) const {
+        line[l] = (T)((double)re * sc);
+        line[l + 1] = (T)((double)im * sc);
+    }
+};
+
+// A tile's span: its first value at `p`, the 16-byte-aligned address at or
+// below it and the 8-byte words between the two (0 or 1 for FP64).
+struct Span {
+    uintptr_t a0;
+    int off;
+};
+template <typename T>
+__device__ __forceinline__ Span span_at(const T* p) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    return Span{a & ~uintptr_t(15), (int)((a & 15) / sizeof(T))};
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+            saddr(dst)),
+        "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(saddr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void bulk_store(void* dst, const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(
+                     reinterpret_cast<uint64_t>(dst)),
+                 "r"(saddr(src)), "r"(bytes)
+                 : "memory");
+}
+
+// The 16-byte-aligned interior [i0, i1) of the byte range [b0, b1).
+__device__ __forceinline__ void interior(uintptr_t b0, uintptr_t b1, uintptr_t& i0, uintptr_t& i1) {
+    i0 = (b0 + 15) & ~uintptr_t(15);
+    i1 = b1 & ~uintptr_t(15);
+}
+
+// LDM: kLdTensor -- the input moves by 16 x 16 tensor boxes (ldmap, swizzled
+// layout); kLdSpan -- by one bulk copy of the tile's rows (row-major, rows of
+// a.in_su values).  STM: kStTensor -- the output leaves by tensor boxes
+// (stmap); kStRows -- by bulk copies of each row's aligned interior (rows of
+// a.out_su values), scaled by a.scale when a.use_scale.
+template <typename T, int M, int KIND, int LDM, int STM>
 __global__ void __launch_bounds__(XCfg<M>::NT + 32, 1)
 xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUtensorMap stmap, const T* in,
           T* out, PassArgs a, LineTables<T> tg, XGeom g, int ntx, int ntiles, int* flags,
@@ -146,7 +210,7 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
     if (t == 0) {
         *abort = 0;
         for (int s = 0; s < kStages; ++s) {
-            mbar_init(full + s, LD_TMA ? 1 : 32);
+            mbar_init(full + s, 1);
             mbar_init(ready + s, NT);
         }
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -155,79 +219,83 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
 
     const int nloc = (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1;
     auto stage_of = [&](int s) { return reinterpret_cast<T*>(smem_raw + (size_t)s * SL::stage); };
+    // tile i of this CTA: first line ub, plane v, lines nl
+    auto tile_of = [&](int i, int& ub, int& v, int& nl) {
+        const int tile = (int)blockIdx.x + i * (int)gridDim.x;
+        ub = a.u0 + (tile % ntx) * W;
+        v = a.v0 + tile / ntx;
+        nl = min(W, a.u0 + a.nu - ub);
+    };
+    auto in_row0 = [&](int ub, int v) { return in + (long long)v * a.in_sv + (long long)ub * a.in_su; };
+    auto out_row0 = [&](int ub, int v) { return out + (long long)v * a.out_sv + (long long)ub * a.out_su; };
 
     if (t >= NT) {
-        // ---------------- producer warp ----------------
-        const int lane = t - NT;
+        // ---------------- producer (one thread) ----------------
+        if (t != NT) return;
+        if constexpr (LDM == kLdTensor)
+            asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&ldmap)) : "memory");
+        if constexpr (STM == kStTensor)
+            asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&stmap)) : "memory");
         auto issue_load = [&](int i) {
             const int s = i % kStages;
-            const int tile = (int)blockIdx.x + i * (int)gridDim.x;
-            const int ub = a.u0 + (tile % ntx) * W;
-            const int v = a.v0 + tile / ntx;
+            int ub, v, nl;
+            tile_of(i, ub, v, nl);
             T* dst = stage_of(s);
-            if constexpr (LD_TMA) {
-                if (lane == 0) {
-                    mbar_expect_tx(full + s, (uint32_t)(g.ld_nblk * 256 * sizeof(T)));
-                    for (int q = 0; q < g.ld_nblk; ++q) {
-                        const int blk = g.ld_blk0 + q;
-                        tma_load(dst + blk * 256, &ldmap, blk * 16, ub, v, full + s);
-                    }
+            if constexpr (LDM == kLdTensor) {
+                mbar_expect_tx(full + s, (uint32_t)(g.ld_nblk * 256 * sizeof(T)));
+                for (int q = 0; q < g.ld_nblk; ++q) {
+                    const int blk = g.ld_blk0 + q;
+                    tma_load(dst + blk * 256, &ldmap, blk * 16, ub, v, full + s);
                 }
             } else {
-                const int nl = min(W, a.u0 + a.nu - ub);
-                for (int r = 0; r < W; ++r) {
-                    const bool ok = r < nl;
-                    const T* row = in + (long long)v * a.in_sv + (long long)(ok ? ub + r : ub) * a.in_su;
-                    for (int l = LO + lane; l <= HI; l += 32) {
-                        const bool valid = ok && l >= a.ld_lo && l <= a.ld_hi;
-                        cp_async_elem<sizeof(T)>(dst + swz(l, r), valid ? row + l : in, valid);
-                    }
-                }
-                cp_async_arrive_noinc(full + s);
+                // rows ub .. ub + nl - 1, whole, as one span widened to 16 bytes
+                const T* p0 = in_row0(ub, v);
+                const Span sp = span_at(p0);
+                const uintptr_t end = (reinterpret_cast<uintptr_t>(p0 + (long long)nl * a.in_su) + 15) &
+                                      ~uintptr_t(15);
+                const uint32_t bytes = (uint32_t)(end - sp.a0);
+                mbar_expect_tx(full + s, bytes);
+                bulk_load(dst, reinterpret_cast<const void*>(sp.a0), bytes, full + s);
             }
         };
-        if (!LD_TMA || !ST_TMA || lane == 0) {
-            if (LD_TMA && lane == 0) {
-                asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&ldmap)) : "memory");
-            }
-            if (ST_TMA && lane == 0) {
-                asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&stmap)) : "memory");
-            }
-            const int pre = nloc < kStages ? nloc : kStages;
-            for (int i = 0; i < pre; ++i) issue_load(i);
-            for (int i = 0; i < nloc; ++i) {
-                const int s = i % kStages;
-                if (!mbar_wait(ready + s, (uint32_t)((i / kStages) & 1), abort, wait_limit))
-                    atomicOr(flags, tma::kFlagProducer);
-                if constexpr (ST_TMA) {
-                    if (lane == 0) {
-                        const int tile = (int)blockIdx.x + i * (int)gridDim.x;
-                        const int ub = a.u0 + (tile % ntx) * W;
-                        const int v = a.v0 + tile / ntx;
-                        const T* src = stage_of(s);
-                        for (int q = 0; q < g.st_nblk; ++q) {
-                            const int blk = g.st_blk0 + q;
-                            tma_store(&stmap, blk * 16, ub, v, src + blk * 256);
-                        }
-                        asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
-                    }
+        const int pre = nloc < kStages ? nloc : kStages;
+        for (int i = 0; i < pre; ++i) issue_load(i);
+        for (int i = 0; i < nloc; ++i) {
+            const int s = i % kStages;
+            if (!mbar_wait(ready + s, (uint32_t)((i / kStages) & 1), abort, wait_limit))
+                atomicOr(flags, tma::kFlagProducer);
+            int ub, v, nl;
+            tile_of(i, ub, v, nl);
+            const T* src = stage_of(s);
+            if constexpr (STM == kStTensor) {
+                for (int q = 0; q < g.st_nblk; ++q) {
+                    const int blk = g.st_blk0 + q;
+                    tma_store(&stmap, blk * 16, ub, v, src + blk * 256);
                 }
-                if (i + kStages < nloc) {
-                    if constexpr (ST_TMA) {
-                        if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
-                    }
-                    if constexpr (!LD_TMA) __syncwarp();
-                    issue_load(i + kStages);
+            } else {
+                // aligned interiors of the rows' output windows (the ends are
+                // stored by the compute threads)
+                T* p0 = out_row0(ub, v);
+                const uintptr_t base = reinterpret_cast<uintptr_t>(p0) & ~uintptr_t(15);
+                const unsigned char* sb = reinterpret_cast<const unsigned char*>(src);
+                const bool whole = a.st_lo == 0 && a.st_hi == a.out_su - 1;
+                for (int r = 0; r < (whole ? 1 : nl); ++r) {
+                    const T* q0 = p0 + (long long)r * a.out_su + a.st_lo;
+                    const T* q1 = whole ? p0 + (long long)nl * a.out_su : p0 + (long long)r * a.out_su + a.st_hi + 1;
+                    uintptr_t i0, i1;
+                    interior(reinterpret_cast<uintptr_t>(q0), reinterpret_cast<uintptr_t>(q1), i0, i1);
+                    if (i1 > i0) bulk_store(reinterpret_cast<void*>(i0), sb + (i0 - base), (uint32_t)(i1 - i0));
                 }
             }
-            if constexpr (ST_TMA) {
-                if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
-            }
-            if constexpr (!LD_TMA) asm volatile("cp.async.wait_all;\n" ::: "memory");
-            if constexpr (LD_TMA) {
-                if (lane == 0) tma::drain_loads(full, nloc, kStages, wait_limit, flags);
+            asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+            if (i + kStages < nloc) {
+                // the buffer is refilled once the stores have read it
+                asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+                issue_load(i + kStages);
             }
         }
+        asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+        tma::drain_loads(full, nloc, kStages, wait_limit, flags);
         return;
     }
 
@@ -241,20 +309,22 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
             if (t == 0) atomicOr(flags, tma::kFlagConsumer);
         }
         T* buf = stage_of(s);
-        const int tile = (int)blockIdx.x + i * (int)gridDim.x;
-        const int ub = a.u0 + (tile % ntx) * W;
-        const int v = a.v0 + tile / ntx;
-        const int nl = min(W, a.u0 + a.nu - ub);
+        int ub, v, nl;
+        tile_of(i, ub, v, nl);
+        const int off = (LDM == kLdSpan) ? span_at(in_row0(ub, v)).off : 0;
+        // entry l of line r of the loaded real view
+        auto at = [&](int l, int r) -> T& {
+            if constexpr (LDM == kLdSpan) return buf[off + r * (int)a.in_su + l];
+            else return buf[swz(l, r)];
+        };
         bool fix = false;
-        if constexpr (LD_TMA) {
-            // entries of the kind's input window outside the load window are 0
-            if (LO < a.ld_lo || HI > a.ld_hi) {
-                for (int e = t; e < W * (HI - LO + 1); e += NT) {
-                    const int r = e % W, l = LO + e / W;
-                    if (l < a.ld_lo || l > a.ld_hi) buf[swz(l, r)] = T(0);
-                }
-                fix = true;
+        // entries of the kind's input window outside the load window are 0
+        if (LO < a.ld_lo || HI > a.ld_hi) {
+            for (int e = t; e < W * (HI - LO + 1); e += NT) {
+                const int r = e % W, l = LO + e / W;
+                if (l < a.ld_lo || l > a.ld_hi) at(l, r) = T(0);
             }
+            fix = true;
         }
         if (a.has_bc) {
             // boundary terms: every entry of a row on a y or z boundary, else
@@ -264,33 +334,53 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
             for (int r = 0; r < nl; ++r) {
                 const int j = ub + r;
                 if (!(zrow || j == b.ys || j == b.ye)) continue;
-                for (int l = a.ld_lo + t; l <= a.ld_hi; l += NT)
-                    buf[swz(l, r)] = (T)bc_terms((double)buf[swz(l, r)], b, l, j, v);
+                for (int l = a.ld_lo + t; l <= a.ld_hi; l += NT) at(l, r) = (T)bc_terms((double)at(l, r), b, l, j, v);
             }
             for (int e = t; e < 2 * nl; e += NT) {
                 const int r = e >> 1, j = ub + r;
                 if (zrow || j == b.ys || j == b.ye) continue;
                 if ((e & 1) && b.xe == b.xs) continue;
                 const int l = (e & 1) ? b.xe : b.xs;
-                buf[swz(l, r)] = (T)bc_terms((double)buf[swz(l, r)], b, l, j, v);
+                at(l, r) = (T)bc_terms((double)at(l, r), b, l, j, v);
             }
             fix = true;
         }
         if (fix) CF::sync();
-        SwzSink<T> sink{buf, c};
-        transform_lines<T, CF, KIND>(buf, red, c, slot, tb, sink);
-        if constexpr (ST_TMA) {
-            // make this thread's writes visible to the tensor store, then release
-            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        } else {
-            // each warp stores rows r = 2w, 2w + 1: 32 consecutive entries per instruction
-            const int lane = t & 31, wq = t >> 5;
-            for (int r = wq; r < W; r += NT / 32) {
-                if (r >= nl) continue;
-                T* row = out + (long long)v * a.out_sv + (long long)(ub + r) * a.out_su;
-                for (int l = a.st_lo + lane; l <= a.st_hi; l += 32) row[l] = (T)((double)buf[swz(l, r)] * sc);
+        T* outp = nullptr;
+        int offo = 0;
+        if constexpr (STM == kStRows) {
+            outp = out_row0(ub, v);
+            offo = span_at(outp).off;
+        }
+        auto run = [&](const auto& X) {
+            if constexpr (STM == kStTensor) {
+                SwzSink<T> sink{buf, c};
+                transform_lines_v<T, CF, KIND>(X, buf, red, c, slot, tb, sink);
+            } else {
+                RowSink<T> sink{buf + offo + c * (int)a.out_su, sc};
+                transform_lines_v<T, CF, KIND>(X, buf, red, c, slot, tb, sink);
+            }
+        };
+        if constexpr (LDM == kLdSpan) run(RowView<T>{buf + off + c * (int)a.in_su});
+        else run(CF::reader(static_cast<const T*>(buf), c));
+        if constexpr (STM == kStRows) {
+            // the 8-byte ends of the rows' windows that the aligned bulk
+            // stores leave out: (row, side) per thread
+            const bool whole = a.st_lo == 0 && a.st_hi == a.out_su - 1;
+            const int nrow = whole ? 1 : nl;
+            for (int e = t; e < 2 * nrow; e += NT) {
+                const int r = e >> 1;
+                const int rl = (whole && (e & 1)) ? nl - 1 : r;          // row of the end
+                const int l = (e & 1) ? a.st_hi : a.st_lo;
+                T* q = outp + (long long)rl * a.out_su + l;
+                const uintptr_t qa = reinterpret_cast<uintptr_t>(q);
+                // left end: not on a 16-byte boundary; right end: its end not on one
+                const bool edge = (e & 1) ? ((qa + sizeof(T)) & 15) != 0 : (qa & 15) != 0;
+                if (edge) *q = buf[offo + rl * (int)a.out_su + l];
             }
         }
+        // make this thread's writes visible to the bulk / tensor stores, then release
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         mbar_arrive(ready + s);
     }
 }

@@ -226,6 +226,40 @@ int chz_helmholtz_solve_noalloc(double left, double right, int nx, int xbc,
                                 const double* bcf, const double* bce,
                                 double lambda, double* f, void* stream);
 
+/* Slab-decomposed solve over several GPUs (no counterpart in the reference,
+ * whose solver runs on one GPU): f is split into slabs of whole z planes, the
+ * rank of slab r holding planes [z0, z0 + nzl) as a contiguous array
+ * (nzl (NY+1)(NX+1) doubles), and one solve is
+ *   1. chz_slab_forward on every rank: x and y forward passes (boundary terms
+ *      applied) of the slab's planes inside the z unknown window, f_slab ->
+ *      ws_slab (nzl (NY+2)(NX+2) doubles, 256-byte aligned;
+ *      chz_slab_work_elems), plane k of the slab at ws_slab + (k - z0)(NY+2)(NX+2);
+ *   2. an all-to-all: the rank of y-row block [j0, j0 + nj) of the spectral y
+ *      window receives those rows of every unknown z plane, as the pencil
+ *      (Ze - Zs + 1) x nj x (NX+2) doubles, [k - Zs][j - j0][x];
+ *   3. chz_slab_z on every rank: the fused z pass (forward, eigenvalue
+ *      division, inverse) on its pencil (256-byte aligned);
+ *   4. the reverse all-to-all into ws_slab;
+ *   5. chz_slab_inverse on every rank: y and x inverse passes, ws_slab ->
+ *      f_slab, scaled as the solve, plus the x and y periodic copies;
+ *   6. with a periodic z axis, plane NZ <- plane 0 (across slabs: the caller's).
+ * The exchanges are the caller's (cuhelmholtz_b200.slab does them over
+ * torch.distributed).  The slab holding the first (last) unknown z plane of a
+ * Dirichlet z face must hold plane 0 (NZ), whose values the boundary terms
+ * read.  Face arrays are the whole problem's.  The result equals
+ * chz_helmholtz_solve's on the whole grid.  Stream-ordered. */
+int chz_slab_forward(double left, double right, int nx, int xbc, const double* bcl, const double* bcr,
+                     double bottom, double top, int ny, int ybc, const double* bcb, const double* bct,
+                     double front, double back, int nz, int zbc, const double* bcf, const double* bce,
+                     const double* f_slab, int z0, int nzl, double* ws_slab, void* stream);
+int chz_slab_z(double left, double right, int nx, int xbc, double bottom, double top, int ny, int ybc,
+               double front, double back, int nz, int zbc, double lambda, double* pencil, int j0, int nj,
+               void* stream);
+int chz_slab_inverse(double left, double right, int nx, int xbc, double bottom, double top, int ny, int ybc,
+                     double front, double back, int nz, int zbc, double* ws_slab, double* f_slab, int z0,
+                     int nzl, void* stream);
+size_t chz_slab_work_elems(int nx, int ny, int nzl);
+
 /* Releases the library-owned workspaces and cached tables of the current
  * device (after synchronising it). */
 int chz_release_cached(void);
