@@ -352,17 +352,33 @@ template <typename T>
 struct StridedView {
     const T* __restrict__ R;
     int PR, c;
+    static constexpr bool kPair = false;   // entries l, l + 1 are not adjacent
     __device__ __forceinline__ T operator()(int l) const { return R[l * PR + c]; }
+    __device__ __forceinline__ C2<T> pair(int l) const { return mk<T>(R[l * PR + c], R[(l + 1) * PR + c]); }
 };
 
 template <typename T>
 __device__ __forceinline__ C2<T> inv_spectrum(int kind, const T* __restrict__ R, int PR, int c,
                                               int k, int N, int M, const LineTables<T>& tb);
 
-// The same on any real-view accessor V (entry l of the line: V(l)).
+// The same on any real-view accessor V (entry l of the line: V(l)).  A view
+// whose entries 2j, 2j + 1 share one aligned 16-byte word (V::kPair) is read a
+// pair at a time where the kind takes both (one shared-memory access instead
+// of two; the DCT-I / DST-I differences read pair j - 1 as well).
 template <typename T, typename V>
 __device__ __forceinline__ C2<T> inv_spectrum_v(int kind, const V& X, int k, int N, int M,
                                                 const LineTables<T>& tb) {
+    if constexpr (V::kPair) {
+        if (kind == kC2R && k != 0 && k != M) return X.pair(2 * k);
+        if (kind == kDCT1 && k != 0 && k != M) {
+            const C2<T> p1 = X.pair(2 * k), p0 = X.pair(2 * k - 2);
+            return mk<T>(p1.x, p0.y - p1.y);
+        }
+        if (kind == kDST1 && k != 0 && k != M) {
+            const C2<T> p1 = X.pair(2 * k), p0 = X.pair(2 * k - 2);
+            return mk<T>(p1.y - p0.y, -p1.x);
+        }
+    }
     switch (kind) {
         case kC2R: {
             if (k == 0 || k == M) return mk<T>(X(2 * k), T(0));

@@ -153,7 +153,9 @@ __device__ __forceinline__ void stage_compute(C2<T>* v, int slot, const C2<T>* _
 template <typename T, int KIND, int M, typename V>
 __device__ __forceinline__ C2<T> pre_value(const V& X, int n, const LineTables<T>& tb) {
     constexpr int N = 2 * M;
-    if constexpr (KIND == kR2C || KIND == kDCT2 || KIND == kDST2) {
+    if constexpr (KIND == kR2C && V::kPair) {
+        return X.pair(2 * n);
+    } else if constexpr (KIND == kR2C || KIND == kDCT2 || KIND == kDST2) {
         return mk<T>(fwd_gather_v<T>(KIND, X, 2 * n, N, M), fwd_gather_v<T>(KIND, X, 2 * n + 1, N, M));
     } else {
         const C2<T> vk = inv_spectrum_v<T>(KIND, X, n, N, M, tb);
@@ -203,6 +205,11 @@ struct OutSink {
         Rv[l * PR + c] = re;
         Rv[(l + 1) * PR + c] = im;
     }
+    // Two adjacent entries, each with its own eigenvalue.
+    __device__ __forceinline__ void put2(int l, T a, T b) const {
+        put(l, a);
+        put(l + 1, b);
+    }
     // put_pair's division applied to a bin held in registers.
     __device__ __forceinline__ void div_pair(int l, C2<T>& v) const {
         if (l >= dlo && l + 1 <= dhi) {
@@ -237,7 +244,10 @@ __device__ __forceinline__ void transform_lines_v(const V& X, T* buf, T* red, in
     T acc = T(0);
     if constexpr (KIND == kDCT1) {
 #pragma unroll
-        for (int q = 0; q < M / P; ++q) acc += X(2 * (slot + q * P) + 1);
+        for (int q = 0; q < M / P; ++q) {
+            if constexpr (V::kPair) acc += X.pair(2 * (slot + q * P)).y;   // the pre step's own pair reads
+            else acc += X(2 * (slot + q * P) + 1);
+        }
     }
 
     // ---- stage 0: pre step fused into the reads ----
@@ -369,8 +379,7 @@ __device__ __forceinline__ void transform_lines_v(const V& X, T* buf, T* red, in
 #pragma unroll
             for (int k = 0; k < LB::r; ++k) {
                 const int m = LB::out_idx(slot, b, k);
-                sink.put(2 * m, outs[2 * (b * LB::r + k)]);
-                sink.put(2 * m + 1, outs[2 * (b * LB::r + k) + 1]);
+                sink.put2(2 * m, outs[2 * (b * LB::r + k)], outs[2 * (b * LB::r + k) + 1]);
                 if constexpr (KIND == kDCT1) {
                     if (m == 0) sink.put(N, extra);
                 }
@@ -387,8 +396,7 @@ __device__ __forceinline__ void transform_lines_v(const V& X, T* buf, T* red, in
                 const T v0 = z.x, v1 = -z.y;
                 const int e0 = 2 * m, e1 = 2 * m + 1;
                 if constexpr (KIND == kC2R) {
-                    sink.put(e0, v0);
-                    sink.put(e1, v1);
+                    sink.put2(e0, v0, v1);
                 } else if constexpr (KIND == kDCT3) {
                     sink.put(e0 < M ? 2 * e0 : 2 * (N - 1 - e0) + 1, T(0.5) * v0);
                     sink.put(e1 < M ? 2 * e1 : 2 * (N - 1 - e1) + 1, T(0.5) * v1);

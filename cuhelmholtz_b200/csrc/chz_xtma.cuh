@@ -47,8 +47,13 @@ template <typename T>
 struct SwzView {
     const T* __restrict__ line;  // buf + 16 c
     int c7;                      // c mod 8
+    // entries 2j, 2j + 1 are one swizzled 16-byte chunk
+    static constexpr bool kPair = sizeof(T) == 8;
     __device__ __forceinline__ T operator()(int l) const {
         return line[((l >> 4) << 8) + ((((l >> 1) & 7) ^ c7) << 1) + (l & 1)];
+    }
+    __device__ __forceinline__ C2<T> pair(int l) const {   // l even
+        return *reinterpret_cast<const C2<T>*>(line + ((l >> 4) << 8) + ((((l >> 1) & 7) ^ c7) << 1));
     }
 };
 
@@ -81,10 +86,11 @@ struct SwzSink {
     T* buf;
     int c;
     __device__ __forceinline__ void put(int l, T v) const { buf[swz(l, c)] = v; }
+    // l even: entries l, l + 1 are one swizzled 16-byte chunk
     __device__ __forceinline__ void put_pair(int l, T re, T im) const {
-        buf[swz(l, c)] = re;
-        buf[swz(l + 1, c)] = im;
+        *reinterpret_cast<C2<T>*>(buf + swz(l, c)) = mk<T>(re, im);
     }
+    __device__ __forceinline__ void put2(int l, T a, T b) const { put_pair(l, a, b); }
 };
 
 struct XGeom {
@@ -118,7 +124,9 @@ enum XStore { kStTensor = 0, kStRows = 1 };
 template <typename T>
 struct RowView {
     const T* __restrict__ line;
+    static constexpr bool kPair = false;   // a row may start on either 8-byte phase
     __device__ __forceinline__ T operator()(int l) const { return line[l]; }
+    __device__ __forceinline__ C2<T> pair(int l) const { return mk<T>(line[l], line[l + 1]); }
 };
 
 // Output sink of the row-major view (row stores), scaled as it is written.
@@ -131,6 +139,7 @@ struct RowSink {
         line[l] = (T)((double)re * sc);
         line[l + 1] = (T)((double)im * sc);
     }
+    __device__ __forceinline__ void put2(int l, T a, T b) const { put_pair(l, a, b); }
 };
 
 // A tile's span: its first value at `p`, the 16-byte-aligned address at or
