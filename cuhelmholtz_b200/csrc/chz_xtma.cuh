@@ -314,12 +314,32 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
     const double sc = a.use_scale ? a.scale : 1.0;
     for (int i = 0; i < nloc; ++i) {
         const int s = i % kStages;
+        int ub, v, nl;
+        tile_of(i, ub, v, nl);
+        // The boundary terms at xs and xe of the tile's rows off the y and z
+        // boundaries (one (row, side) per thread) only read global memory
+        // (faces of f, Neumann arrays): issued before the tile's copy is
+        // waited for, so their latency hides behind it.  They are additive
+        // (bc_terms(v) = v + bc_terms(0) for a single term).
+        double bterm = 0.0;
+        int brow = -1, bl = 0;
+        bool bzrow = false;
+        if (a.has_bc) {
+            const BcArgs& b = a.bc;
+            bzrow = (v == b.zs || v == b.ze);
+            if (!bzrow && t < 2 * nl) {
+                const int r = t >> 1, j = ub + r;
+                if (!(j == b.ys || j == b.ye) && !((t & 1) && b.xe == b.xs)) {
+                    bl = (t & 1) ? b.xe : b.xs;
+                    brow = r;
+                    bterm = bc_terms(0.0, b, bl, j, v);
+                }
+            }
+        }
         if (!mbar_wait(full + s, (uint32_t)((i / kStages) & 1), abort, wait_limit)) {
             if (t == 0) atomicOr(flags, tma::kFlagConsumer);
         }
         T* buf = stage_of(s);
-        int ub, v, nl;
-        tile_of(i, ub, v, nl);
         const int off = (LDM == kLdSpan) ? span_at(in_row0(ub, v)).off : 0;
         // entry l of line r of the loaded real view
         auto at = [&](int l, int r) -> T& {
@@ -336,22 +356,15 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
             fix = true;
         }
         if (a.has_bc) {
-            // boundary terms: every entry of a row on a y or z boundary, else
-            // the entries at xs and xe (one (row, side) per thread)
+            // boundary terms: every entry of a row on a y or z boundary (read
+            // here), else the prefetched term at xs or xe
             const BcArgs& b = a.bc;
-            const bool zrow = (v == b.zs || v == b.ze);
             for (int r = 0; r < nl; ++r) {
                 const int j = ub + r;
-                if (!(zrow || j == b.ys || j == b.ye)) continue;
+                if (!(bzrow || j == b.ys || j == b.ye)) continue;
                 for (int l = a.ld_lo + t; l <= a.ld_hi; l += NT) at(l, r) = (T)bc_terms((double)at(l, r), b, l, j, v);
             }
-            for (int e = t; e < 2 * nl; e += NT) {
-                const int r = e >> 1, j = ub + r;
-                if (zrow || j == b.ys || j == b.ye) continue;
-                if ((e & 1) && b.xe == b.xs) continue;
-                const int l = (e & 1) ? b.xe : b.xs;
-                at(l, r) = (T)bc_terms((double)at(l, r), b, l, j, v);
-            }
+            if (brow >= 0) at(bl, brow) = (T)((double)at(bl, brow) + bterm);
             fix = true;
         }
         if (fix) CF::sync();
