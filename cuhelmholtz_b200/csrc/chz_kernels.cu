@@ -336,13 +336,15 @@ int launch_xtma_kind(int kind, int kind2, const void* in, void* out, const PassA
                      const LineTables<double>& tb, int nv, cudaStream_t stream, const char* label);
 }  // namespace xtma
 
-// FP64 contiguous passes of N = 512 whose input and output rows are both
-// 16-byte aligned (do_transform's padded arrays) go to the TMA-pipelined
-// contiguous kernel; -1 when it does not take the pass.
+// FP64 contiguous passes of N = 256 and 512 go to the TMA-pipelined
+// contiguous kernel (each side by tensor boxes on 16-byte-aligned rows, or by
+// bulk spans / row stores on the solver's f); -1 when it does not take the
+// pass.
 static int try_xtma(const void* in, void* out, const PassArgs& a, const DeviceLineTables& tb, int nv,
                     cudaStream_t stream, const char* label) {
-    if (a.acc || a.kind2 >= 0 || tb.M != 256) return -1;
+    if (a.acc || a.kind2 >= 0 || (tb.M != 256 && tb.M != 128)) return -1;
     const LineTables<double> t = to_tables<double>(tb);
+    if (tb.M == 128) return xtma::launch_xtma_kind<128>(a.kind, a.kind2, in, out, a, t, nv, stream, label);
     return xtma::launch_xtma_kind<256>(a.kind, a.kind2, in, out, a, t, nv, stream, label);
 }
 

@@ -181,7 +181,7 @@ __device__ __forceinline__ void interior(uintptr_t b0, uintptr_t b1, uintptr_t& 
 // (stmap); kStRows -- by bulk copies of each row's aligned interior (rows of
 // a.out_su values), scaled by a.scale when a.use_scale.
 template <typename T, int M, int KIND, int LDM, int STM>
-__global__ void __launch_bounds__(XCfg<M>::NT + 32, 1)
+__global__ void __launch_bounds__(XCfg<M>::NT + 32, (M <= 128 ? 2 : 1))
 xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUtensorMap stmap, const T* in,
           T* out, PassArgs a, LineTables<T> tg, XGeom g, int ntx, int ntiles, int* flags,
           long long wait_limit) {

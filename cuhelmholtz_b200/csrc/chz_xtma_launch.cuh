@@ -113,6 +113,10 @@ int launch_span_tensor_m256(int kind, const double* in, double* out, const PassA
                             const LineTables<double>& tb, int nv, cudaStream_t stream, const char* label);
 int launch_tensor_rows_m256(int kind, const double* in, double* out, const PassArgs& a,
                             const LineTables<double>& tb, int nv, cudaStream_t stream, const char* label);
+int launch_span_tensor_m128(int kind, const double* in, double* out, const PassArgs& a,
+                            const LineTables<double>& tb, int nv, cudaStream_t stream, const char* label);
+int launch_tensor_rows_m128(int kind, const double* in, double* out, const PassArgs& a,
+                            const LineTables<double>& tb, int nv, cudaStream_t stream, const char* label);
 
 template <int M, int LDM, int STM>
 int launch_kinds(int kind, const double* in, double* out, const PassArgs& a, const LineTables<double>& tb, int nv,
@@ -163,14 +167,11 @@ int launch_xtma_kind(int kind, int kind2, const void* in, void* out, const PassA
     const bool ld_tensor = rows_aligned(in, a.in_su, a.in_sv);
     const bool st_tensor = rows_aligned(out, a.out_su, a.out_sv) && !a.use_scale;
     if (ld_tensor && st_tensor) return launch_kinds<M, kLdTensor, kStTensor>(kind, pi, po, a, tb, nv, stream, label);
-    if constexpr (M == 256) {
-        if (!ld_tensor && st_tensor && span_side(in, a.in_su))
-            return launch_span_tensor_m256(kind, pi, po, a, tb, nv, stream, label);
-        if (ld_tensor && !rows_aligned(out, a.out_su, a.out_sv) && span_side(out, a.out_su))
-            return launch_tensor_rows_m256(kind, pi, po, a, tb, nv, stream, label);
-        if (ld_tensor && a.use_scale && span_side(out, a.out_su))
-            return launch_tensor_rows_m256(kind, pi, po, a, tb, nv, stream, label);
-    }
+    auto span = M == 256 ? launch_span_tensor_m256 : launch_span_tensor_m128;
+    auto rows = M == 256 ? launch_tensor_rows_m256 : launch_tensor_rows_m128;
+    if (!ld_tensor && st_tensor && span_side(in, a.in_su)) return span(kind, pi, po, a, tb, nv, stream, label);
+    if (ld_tensor && (!rows_aligned(out, a.out_su, a.out_sv) || a.use_scale) && span_side(out, a.out_su))
+        return rows(kind, pi, po, a, tb, nv, stream, label);
     return -1;
 }
 

@@ -1,4 +1,4 @@
-"""GPU parity of the solver's x passes at N = 512, where the pipelined
+"""GPU parity of the solver's x passes at N = 256 and 512, where the pipelined
 contiguous kernel moves the right-hand side f (rows of N + 1 values, 8-byte
 aligned) as one bulk span per tile and stores the solution rows back with
 bulk copies of their 16-byte-aligned interiors plus plain stores of the ends.
@@ -44,10 +44,11 @@ def _oracle(p):
                             p["f"])
 
 
+@pytest.mark.parametrize("n", [256, 512])
 @pytest.mark.parametrize("phase", [0, 1])
 @pytest.mark.parametrize("xbc,ybc,zbc", [(0, 1, 3), (1, 3, 0), (2, 4, 2), (3, 4, 0), (4, 0, 1)])
-def test_x_pass_512_every_code(xbc, ybc, zbc, phase):
-    p = gen.random_problem(512, 12, 20, xbc, ybc, zbc, -3.0, seed=600 + 10 * xbc + phase)
+def test_x_pass_every_code(xbc, ybc, zbc, phase, n):
+    p = gen.random_problem(n, 12, 20, xbc, ybc, zbc, -3.0, seed=600 + 10 * xbc + phase + n)
     got = _solve(p, phase)
     ref = _oracle(p)
     err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
