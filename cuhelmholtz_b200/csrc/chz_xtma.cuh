@@ -312,30 +312,51 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
     const int c = t % W;
     const int slot = t / W;
     const double sc = a.use_scale ? a.scale : 1.0;
+    // The boundary terms at xs and xe of a tile's rows off the y and z
+    // boundaries (one (row, side) per thread) are one global value each (a
+    // face entry of f or a Neumann array) times a coefficient: the value of
+    // tile i + 1 is loaded while tile i is transformed, so its latency never
+    // stalls the CTA's barrier.  A single term is exactly v + coef * value,
+    // as bc_terms applies it.
+    struct BcNext {
+        int row = -1, l = 0;
+        double coef = 0.0;
+        const double* p = nullptr;
+    };
+    auto bc_next = [&](int i) {
+        BcNext q;
+        if (!a.has_bc || i >= nloc) return q;
+        const BcArgs& b = a.bc;
+        int ub, v, nl;
+        tile_of(i, ub, v, nl);
+        if (v == b.zs || v == b.ze || t >= 2 * nl) return q;
+        const int r = t >> 1, j = ub + r;
+        if (j == b.ys || j == b.ye || ((t & 1) && b.xe == b.xs)) return q;
+        const long long row_f = (long long)v * (b.nx + 1) * (b.ny + 1) + (long long)j * (b.nx + 1);
+        const long long row_face = (long long)v * (b.ny + 1) + j;
+        if (!(t & 1)) {   // i == xs
+            if (b.xbc == 1 || b.xbc == 2) { q.p = b.f + row_f; q.coef = -b.dx2; }
+            else if (b.xbc == 3 || b.xbc == 4) { q.p = b.bcl + row_face; q.coef = 2.0 * b.dx; }
+            q.l = b.xs;
+        } else {          // i == xe
+            if (b.xbc == 1 || b.xbc == 4) { q.p = b.f + row_f + b.nx; q.coef = -b.dx2; }
+            else if (b.xbc == 2 || b.xbc == 3) { q.p = b.bcr + row_face; q.coef = -2.0 * b.dx; }
+            q.l = b.xe;
+        }
+        if (q.p) q.row = r;
+        return q;
+    };
+    BcNext bnext = bc_next(0);
+    double bnext_val = bnext.p ? __ldg(bnext.p) : 0.0;
     for (int i = 0; i < nloc; ++i) {
         const int s = i % kStages;
         int ub, v, nl;
         tile_of(i, ub, v, nl);
-        // The boundary terms at xs and xe of the tile's rows off the y and z
-        // boundaries (one (row, side) per thread) only read global memory
-        // (faces of f, Neumann arrays): issued before the tile's copy is
-        // waited for, so their latency hides behind it.  They are additive
-        // (bc_terms(v) = v + bc_terms(0) for a single term).
-        double bterm = 0.0;
-        int brow = -1, bl = 0;
-        bool bzrow = false;
-        if (a.has_bc) {
-            const BcArgs& b = a.bc;
-            bzrow = (v == b.zs || v == b.ze);
-            if (!bzrow && t < 2 * nl) {
-                const int r = t >> 1, j = ub + r;
-                if (!(j == b.ys || j == b.ye) && !((t & 1) && b.xe == b.xs)) {
-                    bl = (t & 1) ? b.xe : b.xs;
-                    brow = r;
-                    bterm = bc_terms(0.0, b, bl, j, v);
-                }
-            }
-        }
+        const bool bzrow = a.has_bc && (v == a.bc.zs || v == a.bc.ze);
+        const BcNext bcur = bnext;
+        const double bcur_val = bnext_val;
+        bnext = bc_next(i + 1);
+        bnext_val = bnext.p ? __ldg(bnext.p) : 0.0;
         if (!mbar_wait(full + s, (uint32_t)((i / kStages) & 1), abort, wait_limit)) {
             if (t == 0) atomicOr(flags, tma::kFlagConsumer);
         }
@@ -364,7 +385,7 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
                 if (!(bzrow || j == b.ys || j == b.ye)) continue;
                 for (int l = a.ld_lo + t; l <= a.ld_hi; l += NT) at(l, r) = (T)bc_terms((double)at(l, r), b, l, j, v);
             }
-            if (brow >= 0) at(bl, brow) = (T)((double)at(bl, brow) + bterm);
+            if (bcur.row >= 0) at(bcur.l, bcur.row) = (T)((double)at(bcur.l, bcur.row) + bcur.coef * bcur_val);
             fix = true;
         }
         if (fix) CF::sync();
