@@ -447,25 +447,8 @@ tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUte
     constexpr bool REGSPEC = RegSpectrum<T, M, W, KIND, KIND2>::value;
     const int c = t % W;
     const int slot = REGSPEC ? paired_slot<CF::P>(t) : t / W;
-    // fused pass: the x and y eigenvalue terms of this thread's line in tile
-    // i + 1 are loaded while tile i is transformed
-    auto exy_of = [&](int i, double& ex, double& ey) {
-        if constexpr (KIND2 >= 0) {
-            if (i < nloc) {
-                const int tile = (int)blockIdx.x + i * (int)gridDim.x;
-                int col = g.col0 + (tile % ntx) * W + c;
-                col = max(a.u0, min(col, a.u0 + a.nu - 1));
-                ex = __ldg(a.dv.ex + col);
-                ey = __ldg(a.dv.ey + a.v0 + tile / ntx);
-            }
-        }
-    };
-    double ex_next = 0.0, ey_next = 0.0;
-    exy_of(0, ex_next, ey_next);
     for (int i = 0; i < nloc; ++i) {
         const int s = i % kStages;
-        const double ex_cur = ex_next, ey_cur = ey_next;
-        exy_of(i + 1, ex_next, ey_next);
         if (!mbar_wait(full + s, (uint32_t)((i / kStages) & 1), abort, wait_limit)) {
             if (t == 0) atomicOr(flags, kFlagConsumer);
         }
@@ -478,7 +461,7 @@ tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUte
             s1.c = c;
             int col = g.col0 + (tile % ntx) * W + c;
             col = max(a.u0, min(col, a.u0 + a.nu - 1));
-            s1.exy = ex_cur + ey_cur;
+            s1.exy = __ldg(a.dv.ex + col) + __ldg(a.dv.ey + v);
             s1.lam = a.dv.lambda;
             s1.ez = ez_s;
             s1.dlo = a.dv.lo;

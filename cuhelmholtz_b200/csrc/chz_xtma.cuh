@@ -369,12 +369,17 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
         };
         bool fix = false;
         // entries of the kind's input window outside the load window are 0
-        if (LO < a.ld_lo || HI > a.ld_hi) {
-            for (int e = t; e < W * (HI - LO + 1); e += NT) {
-                const int r = e % W, l = LO + e / W;
-                if (l < a.ld_lo || l > a.ld_hi) at(l, r) = T(0);
+        // (only those entries are visited: one or two per line)
+        {
+            const int nlo = a.ld_lo > LO ? a.ld_lo - LO : 0;
+            const int nhi = HI > a.ld_hi ? HI - a.ld_hi : 0;
+            if (nlo + nhi > 0) {
+                for (int e = t; e < W * (nlo + nhi); e += NT) {
+                    const int r = e % W, q = e / W;
+                    at(q < nlo ? LO + q : a.ld_hi + 1 + (q - nlo), r) = T(0);
+                }
+                fix = true;
             }
-            fix = true;
         }
         if (a.has_bc) {
             // boundary terms: every entry of a row on a y or z boundary (read
