@@ -716,6 +716,7 @@ def measure_batch(args, count, steps):
     ms = timed(lambda: plan.solve(fs, faces))
     launches = _lib.launch_count() - l0
     targets, tuned_ms = plan.tiles()
+    schedules = plan.radix_schedules()
     # the same batch with the untuned tile size (4096 values per tile)
     prev = chz.BatchPlan.set_autotune(False)
     try:
@@ -752,7 +753,10 @@ def measure_batch(args, count, steps):
             "points_per_step": npts, "hbm_gbs_model": gbs, "frac_model": gbs / peak,
             "model": "80 B per point (five passes of 16 B)",
             "loop_of_single_solves": {"value": loop_value, "ms_per_step": ms_loop / steps},
+            "launch": "one persistent kernel over a work queue of (pass, problem, tile) items, "
+                      "replayed from a CUDA graph",
             "autotune": {"tile_values_per_pass": targets, "tuned_ms_per_pass": tuned_ms,
+                         "radix_schedule_per_pass": schedules,
                          "untuned_value": count * steps / (ms_plain / 1000.0)},
             "speedup_vs_loop": value / loop_value, "gpu_launches": int(launches),
             "max_rel_err_vs_single_solves": max(errs) if errs else None}

@@ -195,7 +195,8 @@ def helmholtz_solve_refined(left, right, NX, xbc, bcl, bcr,
 
 class BatchPlan:
     """Plan for many independent FP64 solves (sizes, codes, domains, lambdas
-    fixed at creation); ``solve`` runs the whole batch as one graph replay.
+    fixed at creation); ``solve`` runs the whole batch as one graph replay of
+    one persistent launch.
 
     problems: sequence of dicts with keys nx, ny, nz, xbc, ybc, zbc, lam and
     optionally dom (left, right, bottom, top, front, back)."""
@@ -241,6 +242,15 @@ class BatchPlan:
         ms = (ctypes.c_float * 5)()
         _check(_lib.lib().chz_batch_plan_tiles(self._handle, t, ms))
         return list(t), [float(v) for v in ms]
+
+    def radix_schedules(self):
+        """Radix schedule the autotuner chose for each of the five passes (0:
+        8s first, then 4 / 2, then odd primes; 1: reversed; 2: 4s in place
+        of the 8s)."""
+        import ctypes
+        v = (ctypes.c_int * 5)()
+        _check(_lib.lib().chz_batch_plan_radix(self._handle, v))
+        return list(v)
 
     @staticmethod
     def set_autotune(on: bool) -> bool:

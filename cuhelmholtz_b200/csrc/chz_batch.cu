@@ -2,14 +2,23 @@
 // sizes, boundary codes and lambdas solved together.
 //
 // A plan holds, for each of the five line passes, one descriptor per problem
-// (windows, strides, kinds, tables) and the prefix sums of the problems' tile
-// counts.  Each pass is ONE launch over the tiles of all problems: a CTA finds
-// its problem by binary search over the prefix sums and runs the generic
-// line-pass tile body on it.  The periodic planes of all problems are one more
-// launch.  The six launches are captured once into a CUDA graph; every call
-// uploads the problems' array pointers (a small pinned copy) and replays the
-// graph.  Pass p of a problem finishes before pass p+1 starts because the
-// launches are stream-ordered, so no device-side waiting is involved.
+// (windows, strides, kinds, tables, radix schedule) and the prefix sums of the
+// problems' tile counts.  A solve is ONE persistent launch over a device work
+// queue: the items are every tile of pass 0 of every problem, then pass 1, ...,
+// then one periodic-plane item per problem; a CTA takes the next item with an
+// atomic counter, finds its pass and problem by binary search, waits (bounded)
+// until the problem's previous pass has all its tiles done (a per-problem,
+// per-pass completion counter released by the tiles), runs the generic
+// line-pass tile body and releases its own counter.  Items are handed out in
+// pass order and only to running CTAs, so every item waited for is already
+// held by a running CTA: no deadlock, whatever the residency.  The reset of
+// the counters and the launch are captured once into a CUDA graph that every
+// call replays after uploading the problems' array pointers.
+//
+// Tile sizes and radix schedules come from a project-written autotuner: at
+// plan creation each pass is timed over all problems (one launch per pass) at
+// several tile sizes, then at several radix schedules of every length, and the
+// fastest is kept.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -25,6 +34,10 @@
 #include "cuhelmholtz_b200.h"
 
 namespace chz {
+namespace tma {
+int* device_flags();
+long long wait_limit();
+}  // namespace tma
 namespace {
 
 constexpr int kPasses = 5;
@@ -83,11 +96,9 @@ batch_pass(const BatchItem* __restrict__ items, const int* __restrict__ start, i
                                                               local / it.ntx, smem_raw);
 }
 
-// Periodic planes of every problem (one CTA per problem).
-__global__ void batch_fixup(const FixItem* __restrict__ fx, const ProbPtrs* __restrict__ ptrs) {
-    const FixItem q = fx[blockIdx.x];
+// Periodic planes of one problem, by the threads of one CTA.
+__device__ __forceinline__ void fixup_problem(const FixItem& q, double* f) {
     if (!q.px && !q.py && !q.pz) return;
-    double* f = ptrs[blockIdx.x].f;
     const long long sfy = q.nx + 1, sfz = (long long)(q.nx + 1) * (q.ny + 1);
     const long long nX = q.px ? (long long)(q.ny + 1) * (q.nz + 1) : 0;
     const long long nY = q.py ? (long long)(q.nx + 1) * (q.nz + 1) : 0;
@@ -112,7 +123,113 @@ __global__ void batch_fixup(const FixItem* __restrict__ fx, const ProbPtrs* __re
         const int si = (q.px && i == q.nx) ? 0 : i;
         const int sj = (q.py && j == q.ny) ? 0 : j;
         const int sk = (q.pz && k == q.nz) ? 0 : k;
-        f[k * sfz + j * sfy + i] = f[sk * sfz + sj * sfy + si];
+        f[k * sfz + j * sfy + i] = __ldcg(f + sk * sfz + sj * sfy + si);
+    }
+}
+
+// The persistent batched solve.  items[q] / start[q]: pass q's descriptors and
+// tile prefix sums; pass_off[q]: index of pass q's first item in the queue
+// (pass_off[kPasses]: the periodic-plane items, one per problem;
+// pass_off[kPasses + 1]: the end); done[s * kPasses + q]: tiles of problem s's
+// pass q finished; next: the queue head.  done and next start at 0.
+struct PersistArgs {
+    const BatchItem* items[kPasses];
+    const int* start[kPasses];
+    int pass_off[kPasses + 2];
+    const FixItem* fix;
+    const ProbPtrs* ptrs;
+    double* ws;
+    int count;
+    int* done;
+    int* next;
+    int* flags;
+    long long wait_limit;
+};
+
+// The tile body of a contiguous (x) or strided (y, z) pass.
+template <bool CONTIG>
+__device__ __forceinline__ void batch_tile(const double* in, double* out, const PassArgs& a,
+                                        const LineTables<double>& tb, int buf_elems, int bx, int by,
+                                        unsigned char* smem) {
+    line_pass_tile<double, double, double, CONTIG, kRadixAll>(in, out, a, tb, buf_elems, bx, by, smem);
+}
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__global__ void __launch_bounds__(kThreads, 2) batch_persistent(PersistArgs A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_item;
+    __shared__ PassArgs s_args;
+    __shared__ LineTables<double> s_tb;
+    const int total = A.pass_off[kPasses + 1];
+    while (true) {
+        __syncthreads();   // the previous item is finished with s_item and the tile buffers
+        if (threadIdx.x == 0) s_item = atomicAdd(A.next, 1);
+        __syncthreads();
+        const int g = s_item;
+        if (g >= total) break;
+        int q = 0;
+        while (q < kPasses && g >= A.pass_off[q + 1]) ++q;   // q == kPasses: periodic planes
+        int s, local = 0;
+        if (q < kPasses) {
+            local = g - A.pass_off[q];
+            s = find_problem(A.start[q], A.count, local);
+            local -= A.start[q][s];
+        } else {
+            s = g - A.pass_off[kPasses];
+        }
+        // the problem's previous pass must be complete (every one of its
+        // tiles released its counter); bounded wait, then a flag
+        if (q > 0 && threadIdx.x == 0) {
+            const int need = A.start[q - 1][s + 1] - A.start[q - 1][s];
+            const int* cnt = A.done + (long long)s * kPasses + (q - 1);
+            const long long t0 = clock64();
+            while (ld_acquire(cnt) < need) {
+                if (clock64() - t0 > A.wait_limit) {
+                    atomicOr(A.flags, kFlagBatchWait);
+                    break;
+                }
+            }
+        }
+        __syncthreads();
+        __threadfence();   // every thread reads after the acquire
+        const ProbPtrs& p = A.ptrs[s];
+        if (q < kPasses) {
+            const BatchItem& it = A.items[q][s];
+            // the item's pass descriptor, with the problem's pointers, is read
+            // by the tile body from shared memory (not held in registers)
+            if (threadIdx.x == 0) {
+                s_args = it.a;
+                s_tb = it.tb;
+                if (s_args.has_bc) {
+                    s_args.bc.f = p.f;
+                    s_args.bc.bcl = p.face[0];
+                    s_args.bc.bcr = p.face[1];
+                    s_args.bc.bcb = p.face[2];
+                    s_args.bc.bct = p.face[3];
+                    s_args.bc.bcf = p.face[4];
+                    s_args.bc.bce = p.face[5];
+                }
+            }
+            __syncthreads();
+            const double* in = it.in_user ? p.f : A.ws + it.ws_off;
+            double* out = it.out_user ? p.f : A.ws + it.ws_off;
+            if (q == 0 || q == kPasses - 1)
+                batch_tile<true>(in, out, s_args, s_tb, it.buf_elems, local % it.ntx, local / it.ntx, smem_raw);
+            else
+                batch_tile<false>(in, out, s_args, s_tb, it.buf_elems, local % it.ntx, local / it.ntx, smem_raw);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence();   // release the tile's writes with the counter
+                atomicAdd(A.done + (long long)s * kPasses + q, 1);
+            }
+        } else {
+            fixup_problem(A.fix[s], p.f);
+        }
     }
 }
 
@@ -141,6 +258,10 @@ struct chz_batch_plan {
     cudaStream_t graph_stream = nullptr;
     int target[kPasses] = {};            // tile size (values per tile) of each pass
     float tuned_ms[kPasses] = {};        // its measured time (0: not tuned)
+    int plan_variant[kPasses] = {};      // radix schedule chosen for each pass
+    int* counters = nullptr;             // count * kPasses pass counters + the queue head
+    int grid = 0;                        // CTAs of the persistent launch
+    size_t smem_all = 0;                 // its dynamic shared memory
 };
 
 namespace {
@@ -157,6 +278,7 @@ void free_plan(chz_batch_plan* p) {
     if (p->ptrs_d) cudaFree(p->ptrs_d);
     if (p->ptrs_h) cudaFreeHost(p->ptrs_h);
     if (p->ws) cudaFree(p->ws);
+    if (p->counters) cudaFree(p->counters);
     if (p->graph_stream) cudaStreamDestroy(p->graph_stream);
     delete p;
 }
@@ -172,6 +294,7 @@ constexpr size_t kBatchMaxSmem = 110 * 1024;  // two CTAs per SM
 constexpr int kDefaultTarget = 4096;            // values per tile without tuning
 constexpr int kTargets[] = {1024, 2048, 4096, 8192, 16384};
 std::atomic<int> g_autotune{1};
+std::atomic<int> g_force_variant{-1};   // >= 0: every pass uses this radix schedule (untuned)
 
 // Fills the tile-dependent fields of pass q for every problem at tile size
 // `target` (values per tile); returns the launch's tile count and shared memory.
@@ -193,6 +316,48 @@ void materialise(const std::vector<PassTemplate>& tp, bool contig, int target, s
         *smem = std::max(*smem, g.smem_bytes);
     }
     *tiles = start[count];
+}
+
+// Radix schedules the autotuner chooses from, for a complex length M:
+// 0: radix 8s first, then 4 or 2, then the odd primes (factor_radices);
+// 1: the same radices in reverse order (odd primes first);
+// 2: radix 4s (and a 2) in place of the 8s, then the odd primes.
+constexpr int kPlanVariants = 3;
+
+bool radix_variant(int M, int variant, RadixPlan* rp) {
+    RadixPlan base;
+    if (factor_radices(M, &base) != 0) return false;
+    if (variant == 0) {
+        *rp = base;
+        return true;
+    }
+    int r[16];
+    int n = 0;
+    if (variant == 1) {
+        for (int st = base.nst - 1; st >= 0; --st) r[n++] = base.radix(st);
+    } else {
+        int m = M, e2 = 0;
+        while (m % 2 == 0) { m /= 2; ++e2; }
+        while (e2 >= 2) { r[n++] = 4; e2 -= 2; }
+        if (e2 == 1) r[n++] = 2;
+        for (int st = 0; st < base.nst; ++st)
+            if (base.radix(st) % 2) r[n++] = base.radix(st);
+    }
+    if (n > kMaxStages || n > 16) return false;
+    unsigned long long code = 0;
+    for (int i = 0; i < n; ++i) code |= (unsigned long long)r[i] << (4 * i);
+    rp->nst = n;
+    rp->code = code;
+    return true;
+}
+
+// Gives every problem of a pass its length's radix schedule `variant`
+// (problems whose length has no such schedule keep theirs).
+void apply_variant(std::vector<BatchItem>& items, int variant) {
+    for (BatchItem& it : items) {
+        RadixPlan rp;
+        if (radix_variant(it.tb.M, variant, &rp)) it.tb.rp = rp;
+    }
 }
 
 cudaError_t launch_pass(chz_batch_plan* p, int q, cudaStream_t s) {
@@ -275,6 +440,25 @@ bool autotune(chz_batch_plan* p, const std::vector<PassTemplate>* tmpl, const st
         }
         p->target[q] = best_t;
         p->tuned_ms[q] = best / 2.0f;
+        // then the radix schedule at that tile size
+        int best_v = 0;
+        for (int v = 1; ok && v < kPlanVariants; ++v) {
+            std::vector<BatchItem> items;
+            std::vector<int> start;
+            materialise(tmpl[q], p->contig[q], best_t, items, start, &p->tiles[q], &p->smem[q]);
+            apply_variant(items, v);
+            float ms = 0.0f;
+            ok = upload_pass(p, q, items, start) == cudaSuccess && launch_pass(p, q, s) == cudaSuccess &&
+                 cudaEventRecord(e0, s) == cudaSuccess && launch_pass(p, q, s) == cudaSuccess &&
+                 launch_pass(p, q, s) == cudaSuccess && cudaEventRecord(e1, s) == cudaSuccess &&
+                 cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+            if (ok && ms < best) {
+                best = ms;
+                best_v = v;
+            }
+        }
+        p->plan_variant[q] = best_v;
+        p->tuned_ms[q] = best / 2.0f;
     }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
@@ -284,15 +468,61 @@ bool autotune(chz_batch_plan* p, const std::vector<PassTemplate>* tmpl, const st
     return ok;
 }
 
-// Records the six launches of one batched solve on `s`.
-int enqueue(chz_batch_plan* p, cudaStream_t s) {
-    for (int q = 0; q < kPasses; ++q) {
-        const cudaError_t e = launch_pass(p, q, s);
-        if (e != cudaSuccess) return cuda_fail((int)e, "batched pass");
+// Dynamic shared memory and grid of the persistent launch (the largest tile
+// buffer of the five passes; as many CTAs as fit the device).
+cudaError_t prepare_persistent(chz_batch_plan* p) {
+    size_t smem = 0;
+    for (int q = 0; q < kPasses; ++q) smem = std::max(smem, p->smem[q]);
+    static std::mutex mu;
+    static size_t set = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (smem > set) {
+            const cudaError_t e =
+                cudaFuncSetAttribute(batch_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            set = smem;
+        }
     }
-    batch_fixup<<<p->count, 256, 0, s>>>(p->fix_d, p->ptrs_d);
-    const cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail((int)e, "batched periodic planes");
+    int cps = 0, sms = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cps, batch_persistent, kThreads, smem);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device);
+    if (e != cudaSuccess) return e;
+    if (cps < 1) return cudaErrorInvalidConfiguration;
+    int total = p->count;
+    for (int q = 0; q < kPasses; ++q) total += p->tiles[q];
+    p->grid = std::min(total, cps * sms);
+    p->smem_all = smem;
+    return cudaSuccess;
+}
+
+// Records one batched solve on `s`: the reset of the pass counters and the
+// queue head, then the persistent launch.
+int enqueue(chz_batch_plan* p, cudaStream_t s) {
+    PersistArgs A{};
+    int off = 0;
+    for (int q = 0; q < kPasses; ++q) {
+        A.items[q] = p->items_d[q];
+        A.start[q] = p->start_d[q];
+        A.pass_off[q] = off;
+        off += p->tiles[q];
+    }
+    A.pass_off[kPasses] = off;
+    A.pass_off[kPasses + 1] = off + p->count;
+    A.fix = p->fix_d;
+    A.ptrs = p->ptrs_d;
+    A.ws = p->ws;
+    A.count = p->count;
+    A.done = p->counters;
+    A.next = p->counters + (size_t)p->count * kPasses;
+    A.flags = tma::device_flags();
+    A.wait_limit = tma::wait_limit();
+    if (!A.flags) return cuda_fail((int)cudaGetLastError(), "batch wait flags");
+    cudaError_t e = cudaMemsetAsync(p->counters, 0, sizeof(int) * ((size_t)p->count * kPasses + 1), s);
+    if (e != cudaSuccess) return cuda_fail((int)e, "batch counters");
+    batch_persistent<<<p->grid, kThreads, p->smem_all, s>>>(A);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail((int)e, "batched solve");
     return CHZ_SUCCESS;
 }
 
@@ -435,13 +665,19 @@ int chz_batch_plan_create(int count, const int* dims, const int* bcs, const doub
             for (int q = 0; q < kPasses; ++q) {
                 p->target[q] = kDefaultTarget;
                 p->tuned_ms[q] = 0.0f;
+                p->plan_variant[q] = 0;
             }
         }
     }
+    const int forced = g_force_variant.load(std::memory_order_relaxed);
     for (int q = 0; q < kPasses && e == cudaSuccess; ++q) {
+        if (forced >= 0) p->plan_variant[q] = forced;
         materialise(tmpl[q], p->contig[q], p->target[q], items[q], start[q], &p->tiles[q], &p->smem[q]);
+        apply_variant(items[q], p->plan_variant[q]);
         e = upload_pass(p, q, items[q], start[q]);
     }
+    if (e == cudaSuccess) e = cudaMalloc(&p->counters, sizeof(int) * ((size_t)count * kPasses + 1));
+    if (e == cudaSuccess) e = prepare_persistent(p);
     if (e != cudaSuccess) {
         const int st = (e == cudaErrorMemoryAllocation) ? fail(CHZ_ERROR_ALLOC, "batch plan allocation failed")
                                                         : cuda_fail((int)e, "batch plan");
@@ -456,12 +692,23 @@ size_t chz_batch_workspace_bytes(const chz_batch_plan* plan) { return plan ? pla
 
 int chz_batch_set_autotune(int on) { return g_autotune.exchange(on ? 1 : 0); }
 
+int chz_batch_set_radix_schedule(int variant) {
+    if (variant < -1 || variant >= kPlanVariants) return -2;
+    return g_force_variant.exchange(variant);
+}
+
 int chz_batch_plan_tiles(const chz_batch_plan* plan, int* targets, float* ms) {
     if (!plan) return fail(CHZ_ERROR_INVALID_VALUE, "NULL plan");
     for (int q = 0; q < kPasses; ++q) {
         if (targets) targets[q] = plan->target[q];
         if (ms) ms[q] = plan->tuned_ms[q];
     }
+    return CHZ_SUCCESS;
+}
+
+int chz_batch_plan_radix(const chz_batch_plan* plan, int* variants) {
+    if (!plan || !variants) return fail(CHZ_ERROR_INVALID_VALUE, "NULL argument");
+    for (int q = 0; q < kPasses; ++q) variants[q] = plan->plan_variant[q];
     return CHZ_SUCCESS;
 }
 
@@ -484,8 +731,9 @@ int chz_batch_solve(chz_batch_plan* p, double* const* f, const double* const* fa
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail((int)e, "pointer upload");
     if (!p->exec) {
-        // capture the six launches once, on a private stream (the legacy
-        // default stream cannot be captured); the graph replays on any stream
+        // capture the counter reset and the persistent launch once, on a
+        // private stream (the legacy default stream cannot be captured); the
+        // graph replays on any stream
         if (!p->graph_stream) {
             e = cudaStreamCreateWithFlags(&p->graph_stream, cudaStreamNonBlocking);
             if (e != cudaSuccess) return cuda_fail((int)e, "capture stream");
@@ -510,7 +758,7 @@ int chz_batch_solve(chz_batch_plan* p, double* const* f, const double* const* fa
     }
     trace_begin(s, "batch_graph");
     e = cudaGraphLaunch(p->exec, s);
-    for (int q = 0; q < kPasses + 1; ++q) count_launch();
+    count_launch();
     trace_end(s);
     if (e != cudaSuccess) return cuda_fail((int)e, "graph launch");
     return CHZ_SUCCESS;

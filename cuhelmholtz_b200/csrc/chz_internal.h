@@ -8,6 +8,17 @@
 
 namespace chz {
 
+// Bit of the device flag word (chz_tma_host.cu) each kind of bounded wait
+// raises when it runs out.
+enum WaitFlag {
+    kFlagProducer = 1,    // the producer gave up waiting for a finished tile
+    kFlagConsumer = 2,    // a compute thread gave up waiting for a tile load
+    kFlagAlign = 4,       // misaligned shared memory (nothing was started)
+    kFlagDrain = 8,       // a load was still in flight when the CTA ended
+    kFlagSelfTest = 16,   // the wait of chz_wait_selftest ran out (as it should)
+    kFlagBatchWait = 32   // a batch item gave up waiting for its problem's previous pass
+};
+
 // Boundary terms of the reference's _3d_bc{1..4}_ini_{x,y,z}_ kernels
 // (_cuda_helmholtz_.inl:70-227), applied while the first solver pass loads f.
 struct BcArgs {

@@ -124,15 +124,6 @@ __device__ __forceinline__ bool mbar_drain(uint64_t* b, uint32_t parity, long lo
     return true;
 }
 
-// Bit of the device flag word each kind of wait raises when it runs out.
-enum WaitFlag {
-    kFlagProducer = 1,    // the producer gave up waiting for a finished tile
-    kFlagConsumer = 2,    // a compute thread gave up waiting for a tile load
-    kFlagAlign = 4,       // misaligned shared memory (nothing was started)
-    kFlagDrain = 8,       // a load was still in flight when the CTA ended
-    kFlagSelfTest = 16    // the wait of chz_wait_selftest ran out (as it should)
-};
-
 // The producer's drain: for every stage that received loads, the phase of
 // the last load issued into it (tile i of this CTA loads stage i % kStages).
 __device__ __forceinline__ void drain_loads(uint64_t* full, int nloc, int stages, long long limit, int* flags) {

@@ -272,7 +272,7 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
         for (int i = 0; i < nloc; ++i) {
             const int s = i % kStages;
             if (!mbar_wait(ready + s, (uint32_t)((i / kStages) & 1), abort, wait_limit))
-                atomicOr(flags, tma::kFlagProducer);
+                atomicOr(flags, kFlagProducer);
             int ub, v, nl;
             tile_of(i, ub, v, nl);
             const T* src = stage_of(s);
@@ -358,7 +358,7 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
         bnext = bc_next(i + 1);
         bnext_val = bnext.p ? __ldg(bnext.p) : 0.0;
         if (!mbar_wait(full + s, (uint32_t)((i / kStages) & 1), abort, wait_limit)) {
-            if (t == 0) atomicOr(flags, tma::kFlagConsumer);
+            if (t == 0) atomicOr(flags, kFlagConsumer);
         }
         T* buf = stage_of(s);
         const int off = (LDM == kLdSpan) ? span_at(in_row0(ub, v)).off : 0;

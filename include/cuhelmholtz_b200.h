@@ -154,9 +154,12 @@ int chz_helmholtz_adjoint(double left, double right, int nx, int xbc,
  * boundary codes, domains and lambdas (no counterpart in the reference, which
  * solves one problem per call).  The plan precomputes every problem's pass
  * descriptors and a work array for all of them; each chz_batch_solve runs
- * the whole batch as six launches (five line passes over the tiles of all
- * problems, then the periodic planes), captured once into a CUDA graph and
- * replayed on `stream`.
+ * the whole batch as ONE persistent launch over a device work queue (every
+ * tile of the five passes of every problem, pass by pass, then each problem's
+ * periodic planes; an item waits -- bounded -- for its problem's previous
+ * pass), captured once into a CUDA graph with the reset of its counters and
+ * replayed on `stream`.  A wait that runs out is reported by
+ * chz_stream_status.
  *   dims    : 3*count cell counts (nx, ny, nz per problem)
  *   bcs     : 3*count boundary codes 0..4
  *   domains : 6*count extents (left, right, bottom, top, front, back), or
@@ -175,14 +178,26 @@ size_t chz_batch_workspace_bytes(const chz_batch_plan* plan);
 int chz_batch_plan_destroy(chz_batch_plan* plan);
 
 /* Autotuner of the batch plans (on by default): chz_batch_plan_create times
- * every pass over all problems at tile sizes of 1024..16384 values per tile,
- * on scratch stand-ins for the problems' arrays, and keeps the fastest per
- * pass.  Returns the previous setting. */
+ * every pass over all problems (one launch per pass) at tile sizes of
+ * 1024..16384 values per tile, then at the three radix schedules, on scratch
+ * stand-ins for the problems' arrays, and keeps the fastest per pass.
+ * Returns the previous setting. */
 int chz_batch_set_autotune(int on);
 
 /* Tile size chosen for each of the five passes (values per tile; targets[5])
  * and its measured time per launch in ms (ms[5]; 0 when not tuned). */
 int chz_batch_plan_tiles(const chz_batch_plan* plan, int* targets, float* ms);
+
+/* Radix schedule chosen for each of the five passes (variants[5]): 0 radix
+ * 8s first, then 4 or 2, then the odd primes; 1 the same in reverse order; 2
+ * radix 4s (and a 2) in place of the 8s.  The autotuner times the three at
+ * the chosen tile size, per pass, over all problems. */
+int chz_batch_plan_radix(const chz_batch_plan* plan, int* variants);
+
+/* Fixes the radix schedule of plans created afterwards (0..2 as above; -1,
+ * the default, lets the autotuner choose).  Returns the previous setting, or
+ * -2 for an unknown schedule. */
+int chz_batch_set_radix_schedule(int variant);
 
 /* Helmholtz solve with FP32 transforms and FP64 iterative refinement.
  * u0 = S32(b); then up to max_corrections times: r = b - A u in FP64 (the

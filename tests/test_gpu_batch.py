@@ -1,6 +1,7 @@
 """GPU tests of the batched solver (chz_batch_plan_create / chz_batch_solve):
 many problems of uneven sizes, boundary codes and lambdas in one graph replay
-of six launches, checked against one-at-a-time solves and the oracle."""
+of one persistent launch (a device work queue of pass tiles with per-problem
+pass counters), checked against one-at-a-time solves and the oracle."""
 import numpy as np
 import pytest
 import torch
@@ -110,3 +111,51 @@ def test_autotuned_and_default_tiles_agree():
         ua, ub = da[0].cpu().numpy(), db[0].cpu().numpy()
         assert _rel(ua, ub) < 1e-13
         assert _rel(ua, _single(p)) < 1e-12
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2])
+def test_every_radix_schedule_matches_single_solves(variant):
+    """Each radix schedule the autotuner chooses from (8s first; reversed; 4s
+    for 8s) gives the single solves' results, over lengths with radices 2..11."""
+    from cuhelmholtz_b200 import _lib
+    probs = [gen.random_problem(nx, ny, nz, xbc, ybc, zbc, lam, seed=900 + i)
+             for i, (nx, ny, nz, xbc, ybc, zbc, lam) in enumerate(
+                 [(48, 80, 96, 0, 1, 2, -1.0), (112, 40, 64, 3, 4, 0, -2.5), (176, 56, 32, 2, 3, 1, -0.3),
+                  (96, 144, 48, 4, 0, 3, -7.0), (160, 32, 88, 1, 2, 4, -0.05)])]
+    prev = _lib.lib().chz_batch_set_radix_schedule(variant)
+    prev_t = api.BatchPlan.set_autotune(False)
+    try:
+        plan = api.BatchPlan(probs)
+    finally:
+        api.BatchPlan.set_autotune(prev_t)
+        _lib.lib().chz_batch_set_radix_schedule(prev)
+    assert plan.radix_schedules() == [variant] * 5
+    fs, faces = [], []
+    for p in probs:
+        f, fc = _dev(p)
+        fs.append(f)
+        faces.append(fc)
+    plan.solve(fs, faces)
+    api.stream_status()
+    for p, f in zip(probs, fs):
+        ref, rfc = _dev(p)
+        api.solve_problem(p, ref, rfc)
+        torch.cuda.synchronize()
+        err = float(torch.linalg.vector_norm(f - ref) / torch.linalg.vector_norm(ref))
+        assert err < 1e-12, (variant, p["nx"], p["ny"], p["nz"], err)
+    plan.close()
+
+
+def test_batch_is_one_launch_per_solve():
+    from cuhelmholtz_b200 import _lib
+    probs = [gen.random_problem(32 + 16 * (i % 4), 48, 40, i % 5, (i + 2) % 5, (i + 4) % 5, -1.5, seed=950 + i)
+             for i in range(12)]
+    plan = api.BatchPlan(probs)
+    fs, faces = zip(*[_dev(p) for p in probs])
+    plan.solve(list(fs), list(faces))
+    torch.cuda.synchronize()
+    n0 = _lib.launch_count()
+    plan.solve(list(fs), list(faces))
+    api.stream_status()
+    assert _lib.launch_count() - n0 == 1
+    plan.close()
