@@ -226,6 +226,22 @@ __device__ __forceinline__ void r2c_div_c2r_regs(T* buf, int c, int slot, bool p
     // the conjugate sums of o1's).  m = 0 pairs bin 0 with the Nyquist bin M.
     auto pair = [&](int m, C2<T> zk, C2<T> zm, C2<T>& o1, C2<T>& o2) {
         const C2<T> wk = ldtw<T>(tb.twN + m);
+        if (m != 0 && 2 * m >= dv.dlo && 2 * m + 1 <= dv.dhi && N - 2 * m >= dv.dlo && N - 2 * m + 1 <= dv.dhi) {
+            // The split, the two divisions and the pre step compose into one
+            // real-linear map of (zk, zm).  With s = zk + conj zm,
+            // t = zk - conj zm, w = w^m = wr + i wi, dm, dp the reciprocal
+            // eigenvalues of bins m and M - m: X[m] = (s - i w t) / 2,
+            // X[M - m] = conj(s + i w t) / 2, and the pre step of the divided
+            // pair gives (|w| = 1)
+            //   o1 = ((dm + dp) + (dm - dp) wi) conj zk - i (dm - dp) wr zm
+            //   o2 = ((dm + dp) - (dm - dp) wi) conj zm - i (dm - dp) wr zk.
+            const T dm = (T)dv.eig(2 * m), dp = (T)dv.eig(N - 2 * m);
+            const T sum = dm + dp, dif = dm - dp;
+            const T c1 = sum + dif * wk.y, c2 = sum - dif * wk.y, g = dif * wk.x;
+            o1 = mk<T>(c1 * zk.x + g * zm.y, -(c1 * zk.y + g * zm.x));
+            o2 = mk<T>(c2 * zm.x + g * zk.y, -(c2 * zm.y + g * zk.x));
+            return;
+        }
         const C2<T> e = cadd<T>(zk, cconj<T>(zm));
         const C2<T> od = cmul<T>(wk, csub<T>(zk, cconj<T>(zm)));
         C2<T> a = mk<T>(T(0.5) * (e.x + od.y), T(0.5) * (e.y - od.x));    // X[m]
