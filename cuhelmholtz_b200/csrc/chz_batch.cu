@@ -132,9 +132,12 @@ __device__ __forceinline__ void fixup_problem(const FixItem& q, double* f) {
 // (pass_off[kPasses]: the periodic-plane items, one per problem;
 // pass_off[kPasses + 1]: the end); done[s * kPasses + q]: tiles of problem s's
 // pass q finished; next: the queue head.  done and next start at 0.
+constexpr int kChunk = 4;   // queue items a CTA takes at once
+
 struct PersistArgs {
     const BatchItem* items[kPasses];
     const int* start[kPasses];
+    const int* owner;            // problem of every pass tile, by queue index
     int pass_off[kPasses + 2];
     const FixItem* fix;
     const ProbPtrs* ptrs;
@@ -145,14 +148,6 @@ struct PersistArgs {
     int* flags;
     long long wait_limit;
 };
-
-// The tile body of a contiguous (x) or strided (y, z) pass.
-template <bool CONTIG>
-__device__ __forceinline__ void batch_tile(const double* in, double* out, const PassArgs& a,
-                                        const LineTables<double>& tb, int buf_elems, int bx, int by,
-                                        unsigned char* smem) {
-    line_pass_tile<double, double, double, CONTIG, kRadixAll>(in, out, a, tb, buf_elems, bx, by, smem);
-}
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
     int v;
@@ -166,69 +161,72 @@ __global__ void __launch_bounds__(kThreads, 2) batch_persistent(PersistArgs A) {
     __shared__ PassArgs s_args;
     __shared__ LineTables<double> s_tb;
     const int total = A.pass_off[kPasses + 1];
+    int cur_q = -1, cur_s = -1;   // (pass, problem) whose descriptor is in s_args, whose wait is done
     while (true) {
-        __syncthreads();   // the previous item is finished with s_item and the tile buffers
-        if (threadIdx.x == 0) s_item = atomicAdd(A.next, 1);
+        __syncthreads();   // the previous items are finished with s_item
+        if (threadIdx.x == 0) s_item = atomicAdd(A.next, kChunk);
         __syncthreads();
-        const int g = s_item;
-        if (g >= total) break;
-        int q = 0;
-        while (q < kPasses && g >= A.pass_off[q + 1]) ++q;   // q == kPasses: periodic planes
-        int s, local = 0;
-        if (q < kPasses) {
-            local = g - A.pass_off[q];
-            s = find_problem(A.start[q], A.count, local);
-            local -= A.start[q][s];
-        } else {
-            s = g - A.pass_off[kPasses];
-        }
-        // the problem's previous pass must be complete (every one of its
-        // tiles released its counter); bounded wait, then a flag
-        if (q > 0 && threadIdx.x == 0) {
-            const int need = A.start[q - 1][s + 1] - A.start[q - 1][s];
-            const int* cnt = A.done + (long long)s * kPasses + (q - 1);
-            const long long t0 = clock64();
-            while (ld_acquire(cnt) < need) {
-                if (clock64() - t0 > A.wait_limit) {
-                    atomicOr(A.flags, kFlagBatchWait);
-                    break;
+        const int g0 = s_item;
+        if (g0 >= total) break;
+        const int g1 = min(g0 + kChunk, total);
+        for (int g = g0; g < g1; ++g) {
+            int q = 0;
+            while (q < kPasses && g >= A.pass_off[q + 1]) ++q;   // q == kPasses: periodic planes
+            const int s = (q < kPasses) ? __ldg(A.owner + g) : g - A.pass_off[kPasses];
+            if (q != cur_q || s != cur_s) {
+                // the problem's previous pass must be complete (every one of
+                // its tiles released its counter); bounded wait, then a flag
+                if (q > 0 && threadIdx.x == 0) {
+                    const int need = A.start[q - 1][s + 1] - A.start[q - 1][s];
+                    const int* cnt = A.done + (long long)s * kPasses + (q - 1);
+                    const long long t0 = clock64();
+                    while (ld_acquire(cnt) < need) {
+                        if (clock64() - t0 > A.wait_limit) {
+                            atomicOr(A.flags, kFlagBatchWait);
+                            break;
+                        }
+                    }
                 }
-            }
-        }
-        __syncthreads();
-        __threadfence();   // every thread reads after the acquire
-        const ProbPtrs& p = A.ptrs[s];
-        if (q < kPasses) {
-            const BatchItem& it = A.items[q][s];
-            // the item's pass descriptor, with the problem's pointers, is read
-            // by the tile body from shared memory (not held in registers)
-            if (threadIdx.x == 0) {
-                s_args = it.a;
-                s_tb = it.tb;
-                if (s_args.has_bc) {
-                    s_args.bc.f = p.f;
-                    s_args.bc.bcl = p.face[0];
-                    s_args.bc.bcr = p.face[1];
-                    s_args.bc.bcb = p.face[2];
-                    s_args.bc.bct = p.face[3];
-                    s_args.bc.bcf = p.face[4];
-                    s_args.bc.bce = p.face[5];
+                // the item's pass descriptor, with the problem's pointers, is
+                // read by the tile body from shared memory
+                if (q < kPasses && threadIdx.x == 0) {
+                    const ProbPtrs& p = A.ptrs[s];
+                    s_args = A.items[q][s].a;
+                    s_tb = A.items[q][s].tb;
+                    if (s_args.has_bc) {
+                        s_args.bc.f = p.f;
+                        s_args.bc.bcl = p.face[0];
+                        s_args.bc.bcr = p.face[1];
+                        s_args.bc.bcb = p.face[2];
+                        s_args.bc.bct = p.face[3];
+                        s_args.bc.bcf = p.face[4];
+                        s_args.bc.bce = p.face[5];
+                    }
                 }
+                cur_q = q;
+                cur_s = s;
+                __syncthreads();
+                __threadfence();   // every thread reads after the acquire
             }
-            __syncthreads();
-            const double* in = it.in_user ? p.f : A.ws + it.ws_off;
-            double* out = it.out_user ? p.f : A.ws + it.ws_off;
-            if (q == 0 || q == kPasses - 1)
-                batch_tile<true>(in, out, s_args, s_tb, it.buf_elems, local % it.ntx, local / it.ntx, smem_raw);
-            else
-                batch_tile<false>(in, out, s_args, s_tb, it.buf_elems, local % it.ntx, local / it.ntx, smem_raw);
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                __threadfence();   // release the tile's writes with the counter
-                atomicAdd(A.done + (long long)s * kPasses + q, 1);
+            const ProbPtrs& p = A.ptrs[s];
+            if (q < kPasses) {
+                const BatchItem& it = A.items[q][s];
+                const int local = g - A.pass_off[q] - A.start[q][s];
+                const double* in = it.in_user ? p.f : A.ws + it.ws_off;
+                double* out = it.out_user ? p.f : A.ws + it.ws_off;
+                // one tile body for the contiguous (x) and strided (y, z) passes
+                line_pass_tile<double, double, double, kContigRuntime, kRadixAll>(
+                    in, out, s_args, s_tb, it.buf_elems, local % it.ntx, local / it.ntx, smem_raw,
+                    q == 0 || q == kPasses - 1);
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    __threadfence();   // release the tile's writes with the counter
+                    atomicAdd(A.done + (long long)s * kPasses + q, 1);
+                }
+            } else {
+                fixup_problem(A.fix[s], p.f);
+                __syncthreads();
             }
-        } else {
-            fixup_problem(A.fix[s], p.f);
         }
     }
 }
@@ -260,6 +258,7 @@ struct chz_batch_plan {
     float tuned_ms[kPasses] = {};        // its measured time (0: not tuned)
     int plan_variant[kPasses] = {};      // radix schedule chosen for each pass
     int* counters = nullptr;             // count * kPasses pass counters + the queue head
+    int* owner = nullptr;                // problem of every pass tile, by queue index
     int grid = 0;                        // CTAs of the persistent launch
     size_t smem_all = 0;                 // its dynamic shared memory
 };
@@ -279,6 +278,7 @@ void free_plan(chz_batch_plan* p) {
     if (p->ptrs_h) cudaFreeHost(p->ptrs_h);
     if (p->ws) cudaFree(p->ws);
     if (p->counters) cudaFree(p->counters);
+    if (p->owner) cudaFree(p->owner);
     if (p->graph_stream) cudaStreamDestroy(p->graph_stream);
     delete p;
 }
@@ -509,6 +509,7 @@ int enqueue(chz_batch_plan* p, cudaStream_t s) {
     }
     A.pass_off[kPasses] = off;
     A.pass_off[kPasses + 1] = off + p->count;
+    A.owner = p->owner;
     A.fix = p->fix_d;
     A.ptrs = p->ptrs_d;
     A.ws = p->ws;
@@ -677,6 +678,16 @@ int chz_batch_plan_create(int count, const int* dims, const int* bcs, const doub
         e = upload_pass(p, q, items[q], start[q]);
     }
     if (e == cudaSuccess) e = cudaMalloc(&p->counters, sizeof(int) * ((size_t)count * kPasses + 1));
+    if (e == cudaSuccess) {
+        // the problem of every pass tile, in queue order
+        std::vector<int> owner;
+        for (int q = 0; q < kPasses; ++q)
+            for (int i = 0; i < count; ++i)
+                owner.insert(owner.end(), (size_t)(start[q][i + 1] - start[q][i]), i);
+        e = cudaMalloc(&p->owner, sizeof(int) * std::max<size_t>(owner.size(), 1));
+        if (e == cudaSuccess && !owner.empty())
+            e = cudaMemcpy(p->owner, owner.data(), sizeof(int) * owner.size(), cudaMemcpyHostToDevice);
+    }
     if (e == cudaSuccess) e = prepare_persistent(p);
     if (e != cudaSuccess) {
         const int st = (e == cudaErrorMemoryAllocation) ? fail(CHZ_ERROR_ALLOC, "batch plan allocation failed")

@@ -13,10 +13,16 @@ template <typename TI>
 __device__ __forceinline__ double ld_in(const TI* p) { return (double)__ldg(p); }
 
 // Body of one tile (bx, by) of a line pass; shared by the single-problem
-// kernel below and the batched kernel (one launch over many problems).
-template <typename T, typename TI, typename TO, bool CONTIG, int RSET>
+// kernel below and the batched kernels (one launch over many problems).
+// CONTIG: 1 contiguous (x) pass, 0 strided (y, z) pass, kContigRuntime: the
+// argument `contig_rt` says which (one body for both, as the persistent batch
+// kernel runs both kinds of pass).
+constexpr int kContigRuntime = 2;
+template <typename T, typename TI, typename TO, int CONTIG, int RSET>
 __device__ __forceinline__ void line_pass_tile(const TI* in, TO* out, const PassArgs& a, const LineTables<T>& tb,
-                                               int buf_elems, int bx, int by, unsigned char* smem_raw) {
+                                               int buf_elems, int bx, int by, unsigned char* smem_raw,
+                                               bool contig_rt = false) {
+    const bool contig = (CONTIG == kContigRuntime) ? contig_rt : (CONTIG != 0);
     T* buf0 = reinterpret_cast<T*>(smem_raw);
     T* buf1 = buf0 + buf_elems;
     T* red = buf1 + buf_elems;
@@ -39,7 +45,7 @@ __device__ __forceinline__ void line_pass_tile(const TI* in, TO* out, const Pass
         const int len = hi - lo + 1;
         const long long vbase = (long long)v * a.in_sv;
         if constexpr (sizeof(TI) == sizeof(T)) {
-            if (CONTIG) {
+            if (contig) {
                 const int total = len * W;
                 for (int idx = tid; idx < total; idx += nthr) {
                     const int c = idx / len;
@@ -60,7 +66,7 @@ __device__ __forceinline__ void line_pass_tile(const TI* in, TO* out, const Pass
             }
             cp_async_wait_all();
             __syncthreads();
-            if (CONTIG && a.has_bc) {
+            if (contig && a.has_bc) {
                 const int ln = a.ld_hi - a.ld_lo + 1;
                 const int total = ln * nl;
                 for (int idx = tid; idx < total; idx += nthr) {
@@ -71,7 +77,7 @@ __device__ __forceinline__ void line_pass_tile(const TI* in, TO* out, const Pass
                 __syncthreads();
             }
         } else {
-            if (CONTIG) {
+            if (contig) {
                 const int total = len * W;
                 for (int idx = tid; idx < total; idx += nthr) {
                     const int c = idx / len;
@@ -149,7 +155,7 @@ __device__ __forceinline__ void line_pass_tile(const TI* in, TO* out, const Pass
         const int len = hi - lo + 1;
         const long long vbase = (long long)v * a.out_sv;
         const double sc = a.scale;
-        if (CONTIG) {
+        if (contig) {
             const int total = len * W;
             for (int idx = tid; idx < total; idx += nthr) {
                 const int c = idx / len;
