@@ -68,6 +68,7 @@ struct TmaGeom {
     int l_mid;        // 1: map dims (u, l, v); 0: (u, v, l)
     unsigned tx_bytes;  // bytes one tile load delivers
     int col0;         // u of map column 0
+    int v_off;        // v of the maps' first plane (the maps start at the first plane the pass reads)
 };
 
 __device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -412,7 +413,7 @@ tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUte
             const int s = i % kStages;
             const int tile = (int)blockIdx.x + i * (int)gridDim.x;
             const int cx = (tile % ntx) * W;
-            const int v = a.v0 + tile / ntx;
+            const int v = a.v0 + tile / ntx - g.v_off;   // map coordinate
             unsigned char* dst = smem_raw + (size_t)s * sbytes;
             mbar_expect_tx(full + s, g.tx_bytes);
             for (int q = 0; q < g.ld_nch; ++q) {
@@ -430,7 +431,7 @@ tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUte
                 atomicOr(flags, kFlagProducer);
             const int tile = (int)blockIdx.x + i * (int)gridDim.x;
             const int cx = (tile % ntx) * W;
-            const int v = a.v0 + tile / ntx;
+            const int v = a.v0 + tile / ntx - g.v_off;   // map coordinate
             const unsigned char* src = smem_raw + (size_t)s * sbytes;
             for (int q = 0; q < g.st_nch; ++q) {
                 const int l = q * g.st_box;

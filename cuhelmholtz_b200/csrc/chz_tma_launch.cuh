@@ -68,11 +68,26 @@ int launch_one(const T* in, T* out, const PassArgs& a, const LineTables<T>& tb, 
     const T* ld_base = in + col0 + (long long)a.ld_lo * a.in_sl;
     T* st_base = out + col0 + (long long)a.st_lo * a.out_sl;
     if ((reinterpret_cast<uintptr_t>(ld_base) & 15) || (reinterpret_cast<uintptr_t>(st_base) & 15)) return -1;
+    // The maps start at the pass's first plane v0 where that stays 16-byte
+    // aligned: a caller may hand a base moved back by planes it never
+    // addresses (the slab solve), and a tensor map's base must lie in its
+    // allocation.  Otherwise they start at plane 0 of the array.
+    g.v_off = 0;
+    {
+        const T* l2 = ld_base + (long long)a.v0 * a.in_sv;
+        T* s2 = st_base + (long long)a.v0 * a.out_sv;
+        if (!(reinterpret_cast<uintptr_t>(l2) & 15) && !(reinterpret_cast<uintptr_t>(s2) & 15)) {
+            ld_base = l2;
+            st_base = s2;
+            g.v_off = a.v0;
+        }
+    }
+    const int dvm = dv - g.v_off;   // planes the maps cover
     CUtensorMap ldmap, stmap;
     {
         const unsigned long long dl = (unsigned long long)(a.ld_hi - a.ld_lo + 1);
-        const unsigned long long dims[3] = {(unsigned long long)du, l_mid ? dl : (unsigned long long)dv,
-                                            l_mid ? (unsigned long long)dv : dl};
+        const unsigned long long dims[3] = {(unsigned long long)du, l_mid ? dl : (unsigned long long)dvm,
+                                            l_mid ? (unsigned long long)dvm : dl};
         const unsigned long long sl = (unsigned long long)(a.in_sl * ES), sv = (unsigned long long)(a.in_sv * ES);
         const unsigned long long strides[2] = {l_mid ? sl : sv, l_mid ? sv : sl};
         const unsigned box[3] = {(unsigned)W, l_mid ? (unsigned)g.ld_box : 1u, l_mid ? 1u : (unsigned)g.ld_box};
@@ -80,8 +95,8 @@ int launch_one(const T* in, T* out, const PassArgs& a, const LineTables<T>& tb, 
     }
     {
         const unsigned long long dl = (unsigned long long)rows_st;
-        const unsigned long long dims[3] = {(unsigned long long)du, l_mid ? dl : (unsigned long long)dv,
-                                            l_mid ? (unsigned long long)dv : dl};
+        const unsigned long long dims[3] = {(unsigned long long)du, l_mid ? dl : (unsigned long long)dvm,
+                                            l_mid ? (unsigned long long)dvm : dl};
         const unsigned long long sl = (unsigned long long)(a.out_sl * ES), sv = (unsigned long long)(a.out_sv * ES);
         const unsigned long long strides[2] = {l_mid ? sl : sv, l_mid ? sv : sl};
         const unsigned box[3] = {(unsigned)W, l_mid ? (unsigned)g.st_box : 1u, l_mid ? 1u : (unsigned)g.st_box};

@@ -96,6 +96,7 @@ struct SwzSink {
 struct XGeom {
     int ld_blk0, ld_nblk;   // tensor-loaded blocks (LD_TMA)
     int st_blk0, st_nblk;   // tensor-stored blocks (ST_TMA)
+    int v_off;              // v of the maps' first plane
 };
 
 template <typename T, int M>
@@ -254,7 +255,7 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
                 mbar_expect_tx(full + s, (uint32_t)(g.ld_nblk * 256 * sizeof(T)));
                 for (int q = 0; q < g.ld_nblk; ++q) {
                     const int blk = g.ld_blk0 + q;
-                    tma_load(dst + blk * 256, &ldmap, blk * 16, ub, v, full + s);
+                    tma_load(dst + blk * 256, &ldmap, blk * 16, ub, v - g.v_off, full + s);
                 }
             } else {
                 // rows ub .. ub + nl - 1, whole, as one span widened to 16 bytes
@@ -279,7 +280,7 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
             if constexpr (STM == kStTensor) {
                 for (int q = 0; q < g.st_nblk; ++q) {
                     const int blk = g.st_blk0 + q;
-                    tma_store(&stmap, blk * 16, ub, v, src + blk * 256);
+                    tma_store(&stmap, blk * 16, ub, v - g.v_off, src + blk * 256);
                 }
             } else {
                 // aligned interiors of the rows' output windows (the ends are

@@ -43,13 +43,18 @@ int launch_one(const double* in, double* out, const PassArgs& a, const LineTable
     std::memset(&ldmap, 0, sizeof(ldmap));
     std::memset(&stmap, 0, sizeof(stmap));
     const unsigned box[3] = {16u, 16u, 1u};
+    // the maps start at the pass's first plane v0 (16-byte aligned: whole
+    // planes of 16-byte-aligned rows); a caller may hand a base moved back by
+    // planes it never addresses (the slab solve), and a tensor map's base must
+    // lie in its allocation
+    g.v_off = a.v0;
     if (LDM == kLdTensor) {
         g.ld_blk0 = LO >> 4;
         g.ld_nblk = (HI >> 4) - g.ld_blk0 + 1;
         const unsigned long long dims[3] = {(unsigned long long)(a.ld_hi + 1), (unsigned long long)(a.u0 + a.nu),
-                                            (unsigned long long)(a.v0 + nv)};
+                                            (unsigned long long)nv};
         const unsigned long long strides[2] = {(unsigned long long)(a.in_su * 8), (unsigned long long)(a.in_sv * 8)};
-        if (!tma::encode_map_swz(&ldmap, in, dims, strides, box)) return -1;
+        if (!tma::encode_map_swz(&ldmap, in + (long long)a.v0 * a.in_sv, dims, strides, box)) return -1;
     } else {
         // whole rows of the span, row-major: the kind's input window inside a
         // row, and the W rows (plus the span's misalignment) inside a stage
@@ -59,10 +64,10 @@ int launch_one(const double* in, double* out, const PassArgs& a, const LineTable
         g.st_blk0 = a.st_lo >> 4;
         g.st_nblk = (a.st_hi >> 4) - g.st_blk0 + 1;
         const unsigned long long dims[3] = {(unsigned long long)(a.st_hi + 1), (unsigned long long)(a.u0 + a.nu),
-                                            (unsigned long long)(a.v0 + nv)};
+                                            (unsigned long long)nv};
         const unsigned long long strides[2] = {(unsigned long long)(a.out_su * 8),
                                                (unsigned long long)(a.out_sv * 8)};
-        if (!tma::encode_map_swz(&stmap, out, dims, strides, box)) return -1;
+        if (!tma::encode_map_swz(&stmap, out + (long long)a.v0 * a.out_sv, dims, strides, box)) return -1;
     } else {
         // the kind's output window inside a row (the row-major sink writes
         // every entry of it), the W rows inside a stage, 8-byte-aligned rows
