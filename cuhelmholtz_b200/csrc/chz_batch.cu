@@ -157,77 +157,97 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
 
 __global__ void __launch_bounds__(kThreads, 2) batch_persistent(PersistArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ int s_item;
     __shared__ PassArgs s_args;
     __shared__ LineTables<double> s_tb;
+    // The queue state is the same for every thread of the CTA: it lives in
+    // shared memory, so no register stays live across the tile body (whose
+    // FFT stages need all 128 of them).
+    __shared__ int s_g, s_g1;          // current item, end of the taken chunk
+    __shared__ int s_q, s_s;           // its pass (kPasses: periodic planes) and problem
+    __shared__ int s_cur_q, s_cur_s;   // (pass, problem) of the descriptor in s_args
     const int total = A.pass_off[kPasses + 1];
-    int cur_q = -1, cur_s = -1;   // (pass, problem) whose descriptor is in s_args, whose wait is done
+    if (threadIdx.x == 0) {
+        s_g = s_g1 = 0;
+        s_cur_q = s_cur_s = -1;
+    }
     while (true) {
-        __syncthreads();   // the previous items are finished with s_item
-        if (threadIdx.x == 0) s_item = atomicAdd(A.next, kChunk);
         __syncthreads();
-        const int g0 = s_item;
-        if (g0 >= total) break;
-        const int g1 = min(g0 + kChunk, total);
-        for (int g = g0; g < g1; ++g) {
-            int q = 0;
-            while (q < kPasses && g >= A.pass_off[q + 1]) ++q;   // q == kPasses: periodic planes
-            const int s = (q < kPasses) ? __ldg(A.owner + g) : g - A.pass_off[kPasses];
-            if (q != cur_q || s != cur_s) {
-                // the problem's previous pass must be complete (every one of
-                // its tiles released its counter); bounded wait, then a flag
-                if (q > 0 && threadIdx.x == 0) {
-                    const int need = A.start[q - 1][s + 1] - A.start[q - 1][s];
-                    const int* cnt = A.done + (long long)s * kPasses + (q - 1);
-                    const long long t0 = clock64();
-                    while (ld_acquire(cnt) < need) {
-                        if (clock64() - t0 > A.wait_limit) {
-                            atomicOr(A.flags, kFlagBatchWait);
-                            break;
-                        }
-                    }
-                }
-                // the item's pass descriptor, with the problem's pointers, is
-                // read by the tile body from shared memory
-                if (q < kPasses && threadIdx.x == 0) {
-                    const ProbPtrs& p = A.ptrs[s];
-                    s_args = A.items[q][s].a;
-                    s_tb = A.items[q][s].tb;
-                    if (s_args.has_bc) {
-                        s_args.bc.f = p.f;
-                        s_args.bc.bcl = p.face[0];
-                        s_args.bc.bcr = p.face[1];
-                        s_args.bc.bcb = p.face[2];
-                        s_args.bc.bct = p.face[3];
-                        s_args.bc.bcf = p.face[4];
-                        s_args.bc.bce = p.face[5];
-                    }
-                }
-                cur_q = q;
-                cur_s = s;
-                __syncthreads();
-                __threadfence();   // every thread reads after the acquire
+        if (threadIdx.x == 0) {
+            if (s_g >= s_g1) {            // chunk used up: take the next one
+                s_g = atomicAdd(A.next, kChunk);
+                s_g1 = min(s_g + kChunk, total);
             }
-            const ProbPtrs& p = A.ptrs[s];
-            if (q < kPasses) {
-                const BatchItem& it = A.items[q][s];
-                const int local = g - A.pass_off[q] - A.start[q][s];
-                const double* in = it.in_user ? p.f : A.ws + it.ws_off;
-                double* out = it.out_user ? p.f : A.ws + it.ws_off;
-                // one tile body for the contiguous (x) and strided (y, z) passes
-                line_pass_tile<double, double, double, kContigRuntime, kRadixAll>(
-                    in, out, s_args, s_tb, it.buf_elems, local % it.ntx, local / it.ntx, smem_raw,
-                    q == 0 || q == kPasses - 1);
-                __syncthreads();
-                if (threadIdx.x == 0) {
-                    __threadfence();   // release the tile's writes with the counter
-                    atomicAdd(A.done + (long long)s * kPasses + q, 1);
-                }
-            } else {
-                fixup_problem(A.fix[s], p.f);
-                __syncthreads();
+            const int g = s_g;
+            if (g < total) {
+                int q = 0;
+                while (q < kPasses && g >= A.pass_off[q + 1]) ++q;
+                s_q = q;
+                s_s = (q < kPasses) ? __ldg(A.owner + g) : g - A.pass_off[kPasses];
             }
         }
+        __syncthreads();
+        if (s_g >= total) break;
+        if (s_q != s_cur_q || s_s != s_cur_s) {
+            const int q = s_q, s = s_s;
+            // the problem's previous pass must be complete (every one of its
+            // tiles released its counter); bounded wait, then a flag
+            if (q > 0 && threadIdx.x == 0) {
+                const int need = A.start[q - 1][s + 1] - A.start[q - 1][s];
+                const int* cnt = A.done + (long long)s * kPasses + (q - 1);
+                const long long t0 = clock64();
+                while (ld_acquire(cnt) < need) {
+                    if (clock64() - t0 > A.wait_limit) {
+                        atomicOr(A.flags, kFlagBatchWait);
+                        break;
+                    }
+                }
+            }
+            // the item's pass descriptor, with the problem's pointers, staged
+            // in shared memory once per (pass, problem)
+            if (q < kPasses && threadIdx.x == 0) {
+                const ProbPtrs& p = A.ptrs[s];
+                s_args = A.items[q][s].a;
+                s_tb = A.items[q][s].tb;
+                if (s_args.has_bc) {
+                    s_args.bc.f = p.f;
+                    s_args.bc.bcl = p.face[0];
+                    s_args.bc.bcr = p.face[1];
+                    s_args.bc.bcb = p.face[2];
+                    s_args.bc.bct = p.face[3];
+                    s_args.bc.bcf = p.face[4];
+                    s_args.bc.bce = p.face[5];
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                s_cur_q = q;
+                s_cur_s = s;
+            }
+            __threadfence();   // every thread reads after the acquire
+        }
+        if (s_q < kPasses) {
+            const BatchItem& it = A.items[s_q][s_s];
+            const int local = s_g - A.pass_off[s_q] - A.start[s_q][s_s];
+            const double* in = it.in_user ? A.ptrs[s_s].f : A.ws + it.ws_off;
+            double* out = it.out_user ? A.ptrs[s_s].f : A.ws + it.ws_off;
+            // one tile body for the contiguous (x) and strided (y, z) passes
+            // a per-thread copy of the descriptor: read from shared memory by
+            // reference, the tile body's loads of it spill registers
+            const PassArgs a = s_args;
+            const LineTables<double> tbl = s_tb;
+            line_pass_tile<double, double, double, kContigRuntime, kRadixAll>(
+                in, out, a, tbl, it.buf_elems, local % it.ntx, local / it.ntx, smem_raw,
+                s_q == 0 || s_q == kPasses - 1);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence();   // release the tile's writes with the counter
+                atomicAdd(A.done + (long long)s_s * kPasses + s_q, 1);
+            }
+        } else {
+            fixup_problem(A.fix[s_s], A.ptrs[s_s].f);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) ++s_g;
     }
 }
 
