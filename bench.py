@@ -714,9 +714,15 @@ def measure_batch(args, count, steps):
 
     l0 = _lib.launch_count()
     ms = timed(lambda: plan.solve(fs, faces))
-    launches = _lib.launch_count() - l0
+    replays = _lib.launch_count() - l0
+    assert replays == args.warmup + steps, replays
     targets, tuned_ms = plan.tiles()
     schedules = plan.radix_schedules()
+    mode, mode_ms = plan.launch_mode()
+    periodic = any(0 in (p["xbc"], p["ybc"], p["zbc"]) for p in probs)
+    # kernels in one graph replay: the persistent kernel, or five passes and
+    # the periodic planes
+    kernels_per_solve = 1 if mode == 0 else 5 + (1 if periodic else 0)
     # the same batch with the untuned tile size (4096 values per tile)
     prev = chz.BatchPlan.set_autotune(False)
     try:
@@ -753,12 +759,15 @@ def measure_batch(args, count, steps):
             "points_per_step": npts, "hbm_gbs_model": gbs, "frac_model": gbs / peak,
             "model": "80 B per point (five passes of 16 B)",
             "loop_of_single_solves": {"value": loop_value, "ms_per_step": ms_loop / steps},
-            "launch": "one persistent kernel over a work queue of (pass, problem, tile) items, "
-                      "replayed from a CUDA graph",
+            "launch": ("one persistent kernel over a work queue of (pass, problem, tile) items"
+                       if mode == 0 else "one launch per pass over all problems, then the periodic planes")
+                      + ", replayed from a CUDA graph",
+            "launch_form_ms": {"persistent": mode_ms[0], "per_pass": mode_ms[1],
+                               "chosen": "persistent" if mode == 0 else "per_pass"},
             "autotune": {"tile_values_per_pass": targets, "tuned_ms_per_pass": tuned_ms,
                          "radix_schedule_per_pass": schedules,
                          "untuned_value": count * steps / (ms_plain / 1000.0)},
-            "speedup_vs_loop": value / loop_value, "gpu_launches": int(launches),
+            "speedup_vs_loop": value / loop_value, "gpu_launches": int(steps * kernels_per_solve),
             "max_rel_err_vs_single_solves": max(errs) if errs else None}
 
 

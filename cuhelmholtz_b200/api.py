@@ -195,8 +195,9 @@ def helmholtz_solve_refined(left, right, NX, xbc, bcl, bcr,
 
 class BatchPlan:
     """Plan for many independent FP64 solves (sizes, codes, domains, lambdas
-    fixed at creation); ``solve`` runs the whole batch as one graph replay of
-    one persistent launch.
+    fixed at creation); ``solve`` runs the whole batch as one graph replay:
+    one persistent launch over a work queue, or one launch per pass, whichever
+    measured faster at creation (``launch_mode``).
 
     problems: sequence of dicts with keys nx, ny, nz, xbc, ybc, zbc, lam and
     optionally dom (left, right, bottom, top, front, back)."""
@@ -251,6 +252,26 @@ class BatchPlan:
         v = (ctypes.c_int * 5)()
         _check(_lib.lib().chz_batch_plan_radix(self._handle, v))
         return list(v)
+
+    def launch_mode(self):
+        """The plan's launch form (0: one persistent launch; 1: a launch per
+        pass) and the measured ms of one batched solve in each ([0, 0]: not
+        timed)."""
+        import ctypes
+        m = ctypes.c_int()
+        ms = (ctypes.c_float * 2)()
+        _check(_lib.lib().chz_batch_plan_launch(self._handle, ctypes.byref(m), ms))
+        return int(m.value), [float(v) for v in ms]
+
+    @staticmethod
+    def set_launch_mode(mode) -> int:
+        """Fixes the launch form of plans created afterwards (0, 1; None or -1
+        times both, the default); returns the previous setting."""
+        m = -1 if mode is None else int(mode)
+        prev = int(_lib.lib().chz_batch_set_launch_mode(m))
+        if prev == -2:
+            raise ValueError(f"unknown launch form {mode}")
+        return prev
 
     @staticmethod
     def set_autotune(on: bool) -> bool:

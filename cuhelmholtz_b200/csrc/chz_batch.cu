@@ -3,22 +3,23 @@
 //
 // A plan holds, for each of the five line passes, one descriptor per problem
 // (windows, strides, kinds, tables, radix schedule) and the prefix sums of the
-// problems' tile counts.  A solve is ONE persistent launch over a device work
-// queue: the items are every tile of pass 0 of every problem, then pass 1, ...,
-// then one periodic-plane item per problem; a CTA takes the next item with an
-// atomic counter, finds its pass and problem by binary search, waits (bounded)
-// until the problem's previous pass has all its tiles done (a per-problem,
-// per-pass completion counter released by the tiles), runs the generic
-// line-pass tile body and releases its own counter.  Items are handed out in
-// pass order and only to running CTAs, so every item waited for is already
-// held by a running CTA: no deadlock, whatever the residency.  The reset of
-// the counters and the launch are captured once into a CUDA graph that every
+// problems' tile counts.  A solve takes one of two launch forms.  Persistent:
+// ONE launch over a device work queue whose items are every tile of pass 0 of
+// every problem, then pass 1, ..., then one periodic-plane item per problem; a
+// CTA takes the next item with an atomic counter, finds its pass and problem,
+// waits (bounded) until the problem's previous pass has all its tiles done (a
+// per-problem, per-pass completion counter released by the tiles), runs the
+// generic line-pass tile body and releases its own counter.  Items are handed
+// out in pass order and only to running CTAs, so every item waited for is
+// already held by a running CTA: no deadlock, whatever the residency.  Per
+// pass: one launch per pass over all problems' tiles, then one for the
+// periodic planes.  The solve is captured once into a CUDA graph that every
 // call replays after uploading the problems' array pointers.
 //
-// Tile sizes and radix schedules come from a project-written autotuner: at
-// plan creation each pass is timed over all problems (one launch per pass) at
-// several tile sizes, then at several radix schedules of every length, and the
-// fastest is kept.
+// Tile sizes, radix schedules and the launch form come from a project-written
+// autotuner: at plan creation each pass is timed over all problems (one launch
+// per pass) at several tile sizes, then at several radix schedules of every
+// length, then a whole solve in each launch form, and the fastest is kept.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -125,6 +126,13 @@ __device__ __forceinline__ void fixup_problem(const FixItem& q, double* f) {
         const int sk = (q.pz && k == q.nz) ? 0 : k;
         f[k * sfz + j * sfy + i] = __ldcg(f + sk * sfz + sj * sfy + si);
     }
+}
+
+// The periodic planes of every problem, one CTA per problem (the per-pass
+// launch form's last launch).
+__global__ void __launch_bounds__(kThreads) batch_fixup(const FixItem* __restrict__ fix,
+                                                        const ProbPtrs* __restrict__ ptrs) {
+    fixup_problem(fix[blockIdx.x], ptrs[blockIdx.x].f);
 }
 
 // The persistent batched solve.  items[q] / start[q]: pass q's descriptors and
@@ -281,6 +289,9 @@ struct chz_batch_plan {
     int* owner = nullptr;                // problem of every pass tile, by queue index
     int grid = 0;                        // CTAs of the persistent launch
     size_t smem_all = 0;                 // its dynamic shared memory
+    bool periodic = false;               // some problem has a periodic axis
+    int mode = 0;                        // 0: one persistent launch; 1: a launch per pass
+    float mode_ms[2] = {};               // measured solve time of each form (0: not timed)
 };
 
 namespace {
@@ -315,6 +326,7 @@ constexpr int kDefaultTarget = 4096;            // values per tile without tunin
 constexpr int kTargets[] = {1024, 2048, 4096, 8192, 16384};
 std::atomic<int> g_autotune{1};
 std::atomic<int> g_force_variant{-1};   // >= 0: every pass uses this radix schedule (untuned)
+std::atomic<int> g_force_mode{-1};      // >= 0: every plan uses this launch form (untimed)
 
 // Fills the tile-dependent fields of pass q for every problem at tile size
 // `target` (values per tile); returns the launch's tile count and shared memory.
@@ -516,9 +528,22 @@ cudaError_t prepare_persistent(chz_batch_plan* p) {
     return cudaSuccess;
 }
 
-// Records one batched solve on `s`: the reset of the pass counters and the
-// queue head, then the persistent launch.
+// Records one batched solve on `s`.  Persistent form: the reset of the pass
+// counters and the queue head, then the persistent launch.  Per-pass form: the
+// five pass launches, then the periodic planes.
 int enqueue(chz_batch_plan* p, cudaStream_t s) {
+    if (p->mode == 1) {
+        for (int q = 0; q < kPasses; ++q) {
+            const cudaError_t e = launch_pass(p, q, s);
+            if (e != cudaSuccess) return cuda_fail((int)e, "batched pass");
+        }
+        if (p->periodic) {
+            batch_fixup<<<p->count, kThreads, 0, s>>>(p->fix_d, p->ptrs_d);
+            const cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) return cuda_fail((int)e, "batched periodic planes");
+        }
+        return CHZ_SUCCESS;
+    }
     PersistArgs A{};
     int off = 0;
     for (int q = 0; q < kPasses; ++q) {
@@ -545,6 +570,54 @@ int enqueue(chz_batch_plan* p, cudaStream_t s) {
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail((int)e, "batched solve");
     return CHZ_SUCCESS;
+}
+
+// Times a whole solve in each launch form (one warm-up, then two solves timed
+// with CUDA events on a private stream) on scratch stand-ins for the problems'
+// arrays, as the autotuner does, and keeps the faster form.  Which one wins
+// depends on the batch: the persistent launch lets one problem's next pass
+// start while other problems still run the previous one, at the price of the
+// queue's bookkeeping and one tile body for every pass.  Returns false when
+// the scratch cannot be allocated or a launch fails (the persistent form then
+// stays).
+bool choose_launch_mode(chz_batch_plan* p, const std::vector<long long>& ws_off, size_t face_max) {
+    double* fake = nullptr;
+    double* zface = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    bool ok = cudaMalloc(&fake, p->ws_bytes) == cudaSuccess &&
+              cudaMalloc(&zface, face_max * sizeof(double)) == cudaSuccess &&
+              cudaMemset(fake, 0, p->ws_bytes) == cudaSuccess &&
+              cudaMemset(zface, 0, face_max * sizeof(double)) == cudaSuccess &&
+              cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess;
+    if (ok && !p->graph_stream) ok = cudaStreamCreateWithFlags(&p->graph_stream, cudaStreamNonBlocking) == cudaSuccess;
+    if (ok) {
+        for (int i = 0; i < p->count; ++i) {
+            p->ptrs_h[i].f = fake + ws_off[i];
+            for (int k = 0; k < 6; ++k) p->ptrs_h[i].face[k] = zface;
+        }
+        ok = cudaMemcpy(p->ptrs_d, p->ptrs_h, sizeof(ProbPtrs) * p->count, cudaMemcpyHostToDevice) == cudaSuccess;
+    }
+    cudaStream_t s = p->graph_stream;
+    for (int m = 0; ok && m < 2; ++m) {
+        p->mode = m;
+        float ms = 0.0f;
+        ok = enqueue(p, s) == CHZ_SUCCESS && cudaEventRecord(e0, s) == cudaSuccess && enqueue(p, s) == CHZ_SUCCESS &&
+             enqueue(p, s) == CHZ_SUCCESS && cudaEventRecord(e1, s) == cudaSuccess &&
+             cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+        p->mode_ms[m] = ok ? ms / 2.0f : 0.0f;
+    }
+    // a persistent wait that ran out voids the timing (the flag stays for
+    // chz_stream_status to report)
+    if (ok) ok = (chz_debug_flags(0) & kFlagBatchWait) == 0;
+    p->mode = (ok && p->mode_ms[1] < p->mode_ms[0]) ? 1 : 0;
+    if (!ok) p->mode_ms[0] = p->mode_ms[1] = 0.0f;
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (fake) cudaFree(fake);
+    if (zface) cudaFree(zface);
+    g_last_error[0] = 0;
+    cudaGetLastError();
+    return ok;
 }
 
 }  // namespace
@@ -676,12 +749,14 @@ int chz_batch_plan_create(int count, const int* dims, const int* bcs, const doub
     if (e == cudaSuccess) e = cudaMallocHost(&p->ptrs_h, sizeof(ProbPtrs) * count);
     p->ws_bytes = (size_t)ws_total * sizeof(double);
     if (e == cudaSuccess) e = cudaMalloc(&p->ws, p->ws_bytes);
-    if (e == cudaSuccess && g_autotune.load(std::memory_order_relaxed)) {
-        size_t face_max = 1;
-        for (int i = 0; i < count; ++i) {
-            const size_t nx = dims[3 * i], ny = dims[3 * i + 1], nz = dims[3 * i + 2];
-            face_max = std::max(face_max, std::max((ny + 1) * (nz + 1), std::max((nx + 1) * (nz + 1), (nx + 1) * (ny + 1))));
-        }
+    size_t face_max = 1;
+    for (int i = 0; i < count; ++i) {
+        const size_t nx = dims[3 * i], ny = dims[3 * i + 1], nz = dims[3 * i + 2];
+        face_max = std::max(face_max, std::max((ny + 1) * (nz + 1), std::max((nx + 1) * (nz + 1), (nx + 1) * (ny + 1))));
+        p->periodic = p->periodic || p->fix_h[i].px || p->fix_h[i].py || p->fix_h[i].pz;
+    }
+    const bool tune = g_autotune.load(std::memory_order_relaxed) != 0;
+    if (e == cudaSuccess && tune) {
         if (!autotune(p, tmpl, ws_off, face_max)) {
             for (int q = 0; q < kPasses; ++q) {
                 p->target[q] = kDefaultTarget;
@@ -709,6 +784,11 @@ int chz_batch_plan_create(int count, const int* dims, const int* bcs, const doub
             e = cudaMemcpy(p->owner, owner.data(), sizeof(int) * owner.size(), cudaMemcpyHostToDevice);
     }
     if (e == cudaSuccess) e = prepare_persistent(p);
+    if (e == cudaSuccess) {
+        const int fm = g_force_mode.load(std::memory_order_relaxed);
+        if (fm >= 0) p->mode = fm;
+        else if (tune) choose_launch_mode(p, ws_off, face_max);
+    }
     if (e != cudaSuccess) {
         const int st = (e == cudaErrorMemoryAllocation) ? fail(CHZ_ERROR_ALLOC, "batch plan allocation failed")
                                                         : cuda_fail((int)e, "batch plan");
@@ -733,6 +813,21 @@ int chz_batch_plan_tiles(const chz_batch_plan* plan, int* targets, float* ms) {
     for (int q = 0; q < kPasses; ++q) {
         if (targets) targets[q] = plan->target[q];
         if (ms) ms[q] = plan->tuned_ms[q];
+    }
+    return CHZ_SUCCESS;
+}
+
+int chz_batch_set_launch_mode(int mode) {
+    if (mode < -1 || mode > 1) return -2;
+    return g_force_mode.exchange(mode);
+}
+
+int chz_batch_plan_launch(const chz_batch_plan* plan, int* mode, float* ms) {
+    if (!plan) return fail(CHZ_ERROR_INVALID_VALUE, "NULL plan");
+    if (mode) *mode = plan->mode;
+    if (ms) {
+        ms[0] = plan->mode_ms[0];
+        ms[1] = plan->mode_ms[1];
     }
     return CHZ_SUCCESS;
 }
@@ -762,9 +857,9 @@ int chz_batch_solve(chz_batch_plan* p, double* const* f, const double* const* fa
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail((int)e, "pointer upload");
     if (!p->exec) {
-        // capture the counter reset and the persistent launch once, on a
-        // private stream (the legacy default stream cannot be captured); the
-        // graph replays on any stream
+        // capture the solve (the counter reset and the persistent launch, or
+        // the per-pass launches) once, on a private stream (the legacy default
+        // stream cannot be captured); the graph replays on any stream
         if (!p->graph_stream) {
             e = cudaStreamCreateWithFlags(&p->graph_stream, cudaStreamNonBlocking);
             if (e != cudaSuccess) return cuda_fail((int)e, "capture stream");

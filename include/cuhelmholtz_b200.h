@@ -153,12 +153,16 @@ int chz_helmholtz_adjoint(double left, double right, int nx, int xbc,
 /* Batched FP64 solves: `count` independent problems of any supported sizes,
  * boundary codes, domains and lambdas (no counterpart in the reference, which
  * solves one problem per call).  The plan precomputes every problem's pass
- * descriptors and a work array for all of them; each chz_batch_solve runs
- * the whole batch as ONE persistent launch over a device work queue (every
- * tile of the five passes of every problem, pass by pass, then each problem's
- * periodic planes; an item waits -- bounded -- for its problem's previous
- * pass), captured once into a CUDA graph with the reset of its counters and
- * replayed on `stream`.  A wait that runs out is reported by
+ * descriptors and a work array for all of them; each chz_batch_solve replays
+ * on `stream` a CUDA graph captured once, of one of two launch forms:
+ *   0: ONE persistent launch over a device work queue (every tile of the five
+ *      passes of every problem, pass by pass, then each problem's periodic
+ *      planes; an item waits -- bounded -- for its problem's previous pass),
+ *      with the reset of its counters;
+ *   1: one launch per pass over all problems, then one for the periodic
+ *      planes.
+ * The plan times both at creation and keeps the faster
+ * (chz_batch_plan_launch).  A wait that runs out is reported by
  * chz_stream_status.
  *   dims    : 3*count cell counts (nx, ny, nz per problem)
  *   bcs     : 3*count boundary codes 0..4
@@ -198,6 +202,16 @@ int chz_batch_plan_radix(const chz_batch_plan* plan, int* variants);
  * the default, lets the autotuner choose).  Returns the previous setting, or
  * -2 for an unknown schedule. */
 int chz_batch_set_radix_schedule(int variant);
+
+/* Launch form of a plan (*mode: 0 persistent, 1 per pass) and the measured
+ * time of one batched solve in each (ms[2]; 0 when not timed: the autotuner
+ * off or the form fixed by chz_batch_set_launch_mode). */
+int chz_batch_plan_launch(const chz_batch_plan* plan, int* mode, float* ms);
+
+/* Fixes the launch form of plans created afterwards (0 or 1 as above; -1, the
+ * default, times both).  Returns the previous setting, or -2 for an unknown
+ * form. */
+int chz_batch_set_launch_mode(int mode);
 
 /* Helmholtz solve with FP32 transforms and FP64 iterative refinement.
  * u0 = S32(b); then up to max_corrections times: r = b - A u in FP64 (the

@@ -1,7 +1,8 @@
 """GPU tests of the batched solver (chz_batch_plan_create / chz_batch_solve):
 many problems of uneven sizes, boundary codes and lambdas in one graph replay
-of one persistent launch (a device work queue of pass tiles with per-problem
-pass counters), checked against one-at-a-time solves and the oracle."""
+-- of one persistent launch (a device work queue of pass tiles with per-problem
+pass counters) or of one launch per pass, whichever the plan measured faster --
+checked against one-at-a-time solves and the oracle."""
 import numpy as np
 import pytest
 import torch
@@ -158,4 +159,44 @@ def test_batch_is_one_launch_per_solve():
     plan.solve(list(fs), list(faces))
     api.stream_status()
     assert _lib.launch_count() - n0 == 1
+    plan.close()
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_each_launch_form_matches_single_solves(mode):
+    """Both launch forms (0: persistent work queue; 1: a launch per pass, then
+    the periodic planes) give the single solves' results, periodic axes
+    included."""
+    probs = [gen.random_problem(nx, ny, nz, xbc, ybc, zbc, lam, seed=970 + i)
+             for i, (nx, ny, nz, xbc, ybc, zbc, lam) in enumerate(
+                 [(48, 64, 32, 0, 0, 0, -1.0), (96, 40, 56, 1, 0, 3, -4.0), (32, 32, 144, 3, 4, 0, -0.2),
+                  (80, 112, 48, 2, 1, 4, -9.0), (64, 48, 96, 0, 3, 2, -0.6)])]
+    prev = api.BatchPlan.set_launch_mode(mode)
+    try:
+        plan = api.BatchPlan(probs)
+    finally:
+        api.BatchPlan.set_launch_mode(prev)
+    m, ms = plan.launch_mode()
+    assert m == mode and ms == [0.0, 0.0]
+    for _ in range(2):      # two graph replays, each on fresh copies of the right-hand sides
+        fs, faces = zip(*[_dev(p) for p in probs])
+        plan.solve(list(fs), list(faces))
+        api.stream_status()
+    for p, f in zip(probs, fs):
+        ref = _single(p)
+        assert _rel(f.cpu().numpy(), ref) < 1e-13, (mode, p["nx"], p["ny"], p["nz"])
+    plan.close()
+
+
+def test_plan_times_both_launch_forms():
+    probs = gen.config4_problems(count=32, seed=21)
+    plan = api.BatchPlan(probs)
+    m, ms = plan.launch_mode()
+    assert m in (0, 1) and ms[0] > 0 and ms[1] > 0
+    assert ms[m] == min(ms)
+    fs, faces = zip(*[_dev(p) for p in probs])
+    plan.solve(list(fs), list(faces))
+    api.stream_status()
+    for i in (0, 13, 31):
+        assert _rel(fs[i].cpu().numpy(), _single(probs[i])) < 1e-13, i
     plan.close()
