@@ -647,7 +647,7 @@ def run_ours(args):
         "data": "synthetic",
         "config": {"workload": name, "description": rec["description"], "grid": rec["grid"],
                    "bc": rec["bc"], "lambda": rec["lambda"], "batch_per_step": args.batch,
-                   "parallelism": f"replicas x{world}",
+                   "parallelism": f"replicas x{world}", "kernel_family": args.kernel_family,
                    "l2": "inputs larger than L2 (each right-hand side 1 array per problem, "
                          f"{rec['npts'] * 8 / 1e9:.2f} GB each)"},
         "hbm_gbs_solve": rec["hbm_gbs_solve"],
@@ -815,6 +815,9 @@ def main():
                     help="run the batching configuration with this many problems instead")
     ap.add_argument("--refine-corrections", type=int, default=2,
                     help="also time the FP32 + FP64-refinement solve with this many corrections (-1: skip)")
+    ap.add_argument("--kernel-family", default="default",
+                    choices=["default", "generic", "no_tma", "cta_xpass"],
+                    help="kernel family of the solver's passes (cuhelmholtz_b200.api.set_kernel_family)")
     args = ap.parse_args()
     args.sub_workloads = [w for w in args.sub_workloads.split(",") if w]
     for w in args.sub_workloads:
@@ -824,6 +827,9 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.kernel_family != "default":
+        import cuhelmholtz_b200 as chz
+        chz.set_kernel_family(args.kernel_family)
     if args.batch_count > 0:
         return run_batch(args)
     return run_ours(args)
