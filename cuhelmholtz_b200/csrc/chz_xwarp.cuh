@@ -27,22 +27,66 @@
 namespace chz {
 namespace xtma {
 
-// Exchange view of line c of a swizzled tile: Z[m] is the 16-byte chunk
-// holding entries 2m, 2m + 1 of the line.
+// The exchanges of a line transform write bins 16 j + k from lane j and read
+// bins j + 16 k into lane j (and the partners M - m): in a line's own
+// storage both strides would put every lane on one bank.  Bin m is therefore
+// kept at slot m ^ ((m >> 4) & 7) of the line's 16-byte slots -- the low three
+// bits (the bank group of a 16-byte slot in a 128-byte row) mixed with bits
+// 4..6 -- which stays inside the line and spreads either access pattern over
+// all eight bank groups.
+__device__ __forceinline__ int zslot(int m) { return m ^ ((m >> 4) & 7); }
+
+// Exchange view of line c of a swizzled tile: 16-byte slot q of the line is
+// the chunk of its entries 2q, 2q + 1.
 template <typename T>
 struct SwzZ {
     C2<T>* base;  // tile as complex values + 8 c
     int c7;       // c mod 8
-    __device__ __forceinline__ C2<T>& operator[](int m) const { return base[((m >> 3) << 7) + ((m & 7) ^ c7)]; }
+    __device__ __forceinline__ C2<T>& operator[](int m) const {
+        const int q = zslot(m);
+        return base[((q >> 3) << 7) + ((q & 7) ^ c7)];
+    }
 };
 
-// Exchange view of a row-major line: Z[m] from the line's first 16-byte
-// boundary (the line holds at least 2M + 1 entries, so 2M values fit).
+// Exchange view of a row-major line: 16-byte slots from the line's first
+// 16-byte boundary (the line holds at least 2M + 1 entries, so M slots fit).
 template <typename T>
 struct RowZ {
     C2<T>* base;
-    __device__ __forceinline__ C2<T>& operator[](int m) const { return base[m]; }
+    __device__ __forceinline__ C2<T>& operator[](int m) const { return base[zslot(m)]; }
 };
+
+// Butterfly j of stage S taken by lane `slot` as its b-th: j = slot + P b (the
+// reads j + nb k of the lanes of a line are then consecutive for every b).
+template <int M, int S>
+struct WBfly {
+    using BF = fast::Bfly<M, S>;
+    static constexpr int r = BF::r, Ns = BF::Ns, B = BF::B, nb = BF::nb, P = M / fast::kR;
+    __device__ static __forceinline__ int j(int slot, int b) { return slot + P * b; }
+    __device__ static __forceinline__ int in_idx(int slot, int b, int k) { return j(slot, b) + k * nb; }
+    __device__ static __forceinline__ int out_idx(int slot, int b, int k) {
+        const int jj = j(slot, b);
+        const int p = jj & (Ns - 1);
+        return (jj - p) * r + p + k * Ns;
+    }
+};
+
+// Stage twiddles and radix-r butterflies for the WBfly assignment.
+template <typename T, int M, int S>
+__device__ __forceinline__ void stage_compute_w(C2<T>* v, int slot, const C2<T>* __restrict__ twM) {
+    using BF = WBfly<M, S>;
+    constexpr int r = BF::r;
+#pragma unroll
+    for (int b = 0; b < BF::B; ++b) {
+        if constexpr (BF::Ns > 1) {
+            const int p = BF::j(slot, b) & (BF::Ns - 1);
+            constexpr int tstep = M / (BF::Ns * r);
+#pragma unroll
+            for (int k = 1; k < r; ++k) v[b * r + k] = cmul<T>(v[b * r + k], ldtw<T>(twM + p * k * tstep));
+        }
+        fast::dft_r<T, r>(v + b * r);
+    }
+}
 
 // Output sink of one line: entry l goes to row[l] (scaled) when l lies in the
 // output window [lo, hi] and the line exists; an entry pair 2m, 2m + 1 is one
@@ -75,7 +119,6 @@ struct GSink {
 template <typename T, int M, int KIND, typename V, typename ZV, typename SINK>
 __device__ __forceinline__ void line_transform_w(const V& X, const ZV& Z, int slot, const LineTables<T>& tb,
                                                  const SINK& sink) {
-    using fast::Bfly;
     constexpr int R = fast::kR;
     constexpr int P = M / R;
     constexpr int N = 2 * M;
@@ -92,7 +135,7 @@ __device__ __forceinline__ void line_transform_w(const V& X, const ZV& Z, int sl
         }
     }
     {
-        using BF = Bfly<M, 0>;
+        using BF = WBfly<M, 0>;
 #pragma unroll
         for (int k = 0; k < R; ++k) v[k] = fast::pre_value<T, KIND, M>(X, BF::in_idx(slot, 0, k), tb);
     }
@@ -101,25 +144,25 @@ __device__ __forceinline__ void line_transform_w(const V& X, const ZV& Z, int sl
         for (int o = P / 2; o >= 1; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     }
     __syncwarp();   // the real view is read: the storage now holds the exchange view
-    fast::stage_compute<T, M, 0>(v, slot, tb.twM);
+    stage_compute_w<T, M, 0>(v, slot, tb.twM);
 
 #define CHZ_WSTAGE(S)                                                                                    \
     if constexpr (NST > S) {                                                                             \
-        using PB = Bfly<M, S - 1>;                                                                       \
+        using PB = WBfly<M, S - 1>;                                                                       \
         _Pragma("unroll") for (int b = 0; b < PB::B; ++b)                                                \
             _Pragma("unroll") for (int k = 0; k < PB::r; ++k) Z[PB::out_idx(slot, b, k)] = v[b * PB::r + k]; \
         __syncwarp();                                                                                    \
-        using BF = Bfly<M, S>;                                                                           \
+        using BF = WBfly<M, S>;                                                                           \
         _Pragma("unroll") for (int b = 0; b < BF::B; ++b)                                                \
             _Pragma("unroll") for (int k = 0; k < BF::r; ++k) v[b * BF::r + k] = Z[BF::in_idx(slot, b, k)]; \
         __syncwarp();                                                                                    \
-        fast::stage_compute<T, M, S>(v, slot, tb.twM);                                                   \
+        stage_compute_w<T, M, S>(v, slot, tb.twM);                                                   \
     }
     CHZ_WSTAGE(1)
     CHZ_WSTAGE(2)
 #undef CHZ_WSTAGE
 
-    using LB = Bfly<M, NST - 1>;
+    using LB = WBfly<M, NST - 1>;
     if constexpr (FWD || KIND == kDCT1 || KIND == kDST1) {
 #pragma unroll
         for (int b = 0; b < LB::B; ++b)
