@@ -111,7 +111,7 @@ template <int M, int KIND, int LDM>
 int launch_w(const double* in, double* out, const PassArgs& a, const LineTables<double>& tb, int nv,
              cudaStream_t stream, const char* label) {
     using CF = XCfg<M>;
-    using SL = XSmem<double, M>;
+    using SL = XWSmem<double, M>;
     constexpr int W = CF::W, N = CF::N;
     constexpr int LO = fast::InWin<KIND, N>::lo, HI = fast::InWin<KIND, N>::hi;
     if ((long long)SL::total > (long long)tma::max_optin_smem()) return -1;

@@ -71,22 +71,41 @@ struct WBfly {
     }
 };
 
-// Stage twiddles and radix-r butterflies for the WBfly assignment.
+// Stage twiddles and radix-r butterflies for the WBfly assignment.  The
+// lanes of a line run different butterflies, so the last stage (Ns = 16)
+// reads its twiddles w^(p k) from tw2[(k - 1) * 16 + p], a table the kernel
+// lays out once: for each k the 16 lanes read 16 consecutive entries (from
+// twM their stride p k would put up to 16 lanes on one bank).
 template <typename T, int M, int S>
-__device__ __forceinline__ void stage_compute_w(C2<T>* v, int slot, const C2<T>* __restrict__ twM) {
+__device__ __forceinline__ void stage_compute_w(C2<T>* v, int slot, const C2<T>* __restrict__ tw2) {
     using BF = WBfly<M, S>;
     constexpr int r = BF::r;
+    static_assert(BF::Ns == 1 || BF::Ns == 16, "stages of M = 128 and 256");
 #pragma unroll
     for (int b = 0; b < BF::B; ++b) {
         if constexpr (BF::Ns > 1) {
             const int p = BF::j(slot, b) & (BF::Ns - 1);
-            constexpr int tstep = M / (BF::Ns * r);
 #pragma unroll
-            for (int k = 1; k < r; ++k) v[b * r + k] = cmul<T>(v[b * r + k], ldtw<T>(twM + p * k * tstep));
+            for (int k = 1; k < r; ++k) v[b * r + k] = cmul<T>(v[b * r + k], ldtw<T>(tw2 + (k - 1) * 16 + p));
         }
         fast::dft_r<T, r>(v + b * r);
     }
 }
+
+// Shared-memory carve-up of the warp-local pass: xtma_pass's, with the
+// last-stage twiddle table in place of the DCT-I partial sums and one
+// barrier per stage.
+template <typename T, int M>
+struct XWSmem {
+    using BASE = XSmem<T, M>;
+    static constexpr int R1 = WBfly<M, XCfg<M>::NST - 1>::r;
+    static constexpr size_t stage = BASE::stage;
+    static constexpr size_t twM = BASE::twM, twN = BASE::twN, tw4N = BASE::tw4N, inv4sin = BASE::inv4sin;
+    static constexpr size_t tw2 = BASE::red;
+    static constexpr size_t bars = (tw2 + sizeof(C2<T>) * (R1 - 1) * 16 + 15) & ~size_t(15);
+    static constexpr size_t abort = bars + kStages * sizeof(uint64_t);
+    static constexpr size_t total = abort + 16 + 1024;  // + alignment slack
+};
 
 // Output sink of one line: entry l goes to row[l] (scaled) when l lies in the
 // output window [lo, hi] and the line exists; an entry pair 2m, 2m + 1 is one
@@ -118,7 +137,7 @@ struct GSink {
 // odd entries is reduced over the line's lanes by shuffles.
 template <typename T, int M, int KIND, typename V, typename ZV, typename SINK>
 __device__ __forceinline__ void line_transform_w(const V& X, const ZV& Z, int slot, const LineTables<T>& tb,
-                                                 const SINK& sink) {
+                                                 const C2<T>* __restrict__ tw2, const SINK& sink) {
     constexpr int R = fast::kR;
     constexpr int P = M / R;
     constexpr int N = 2 * M;
@@ -144,7 +163,7 @@ __device__ __forceinline__ void line_transform_w(const V& X, const ZV& Z, int sl
         for (int o = P / 2; o >= 1; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     }
     __syncwarp();   // the real view is read: the storage now holds the exchange view
-    stage_compute_w<T, M, 0>(v, slot, tb.twM);
+    stage_compute_w<T, M, 0>(v, slot, tw2);
 
 #define CHZ_WSTAGE(S)                                                                                    \
     if constexpr (NST > S) {                                                                             \
@@ -156,7 +175,7 @@ __device__ __forceinline__ void line_transform_w(const V& X, const ZV& Z, int sl
         _Pragma("unroll") for (int b = 0; b < BF::B; ++b)                                                \
             _Pragma("unroll") for (int k = 0; k < BF::r; ++k) v[b * BF::r + k] = Z[BF::in_idx(slot, b, k)]; \
         __syncwarp();                                                                                    \
-        stage_compute_w<T, M, S>(v, slot, tb.twM);                                                   \
+        stage_compute_w<T, M, S>(v, slot, tw2);                                                   \
     }
     CHZ_WSTAGE(1)
     CHZ_WSTAGE(2)
@@ -278,7 +297,7 @@ __global__ void __launch_bounds__(XCfg<M>::NT, (M <= 128 ? 2 : 1))
 xw_pass(const __grid_constant__ CUtensorMap ldmap, const T* in, T* out, PassArgs a, LineTables<T> tg, XGeom g,
         int ntx, int ntiles, int* flags, long long wait_limit) {
     using CF = XCfg<M>;
-    using SL = XSmem<T, M>;
+    using SL = XWSmem<T, M>;
     constexpr int W = CF::W, NT = CF::NT, N = CF::N, P = CF::P;
     constexpr int LO = fast::InWin<KIND, N>::lo, HI = fast::InWin<KIND, N>::hi;
     extern __shared__ __align__(128) unsigned char smem_dyn[];
@@ -307,6 +326,12 @@ xw_pass(const __grid_constant__ CUtensorMap ldmap, const T* in, T* out, PassArgs
         tb.twN = sN;
         tb.tw4N = s4;
         tb.inv4sin = sI;
+    }
+    // last-stage twiddles by (k, butterfly): w^(p k) of the M-point transform
+    C2<T>* tw2 = reinterpret_cast<C2<T>*>(smem_raw + SL::tw2);
+    for (int i = t; i < (SL::R1 - 1) * 16; i += blockDim.x) {
+        const int k = i / 16 + 1, p = i % 16;
+        tw2[i] = tg.twM[p * k * (M / (16 * SL::R1))];
     }
     if (t == 0) {
         *abort = 0;
@@ -434,10 +459,11 @@ xw_pass(const __grid_constant__ CUtensorMap ldmap, const T* in, T* out, PassArgs
         const GSink<T> sink{orow, a.st_lo, a.st_hi, sc, (reinterpret_cast<uintptr_t>(orow) & 15) == 0, on};
         if constexpr (LDM == kLdSpan) {
             line_transform_w<T, M, KIND>(RowView<T>{buf + e}, RowZ<T>{reinterpret_cast<C2<T>*>(buf + e + (e & 1))},
-                                         slot, tb, sink);
+                                         slot, tb, tw2, sink);
         } else {
             line_transform_w<T, M, KIND>(SwzView<T>{buf + (c << 4), c & 7},
-                                         SwzZ<T>{reinterpret_cast<C2<T>*>(buf) + (c << 3), c & 7}, slot, tb, sink);
+                                         SwzZ<T>{reinterpret_cast<C2<T>*>(buf) + (c << 3), c & 7}, slot, tb, tw2,
+                                         sink);
         }
         // the stage is read: the last warp to finish it refills it with tile
         // i + kStages (every warp counts once per use of the stage)
