@@ -60,7 +60,10 @@ int launch_one(const double* in, double* out, const PassArgs& a, const LineTable
         // row, and the W rows (plus the span's misalignment) inside a stage
         if (HI > a.in_su - 1 || a.in_sv < a.in_su * (a.u0 + a.nu) || W * a.in_su + 2 > CF::BUF) return -1;
     }
-    if (STM == kStTensor) {
+    if (STM == kStDirect) {
+        // the output window inside a row, 8-byte-aligned rows
+        if (a.st_lo < 0 || a.st_hi > a.out_su - 1 || (reinterpret_cast<uintptr_t>(out) & 7)) return -1;
+    } else if (STM == kStTensor) {
         g.st_blk0 = a.st_lo >> 4;
         g.st_nblk = (a.st_hi >> 4) - g.st_blk0 + 1;
         const unsigned long long dims[3] = {(unsigned long long)(a.st_hi + 1), (unsigned long long)(a.u0 + a.nu),
@@ -199,8 +202,9 @@ int launch_w_tensor_m128(int kind, const double* in, double* out, const PassArgs
 int launch_w_span_m128(int kind, const double* in, double* out, const PassArgs& a, const LineTables<double>& tb,
                        int nv, cudaStream_t stream, const char* label);
 
-// 1 (default): the contiguous passes at M = 128 and 256 take the warp-local
-// form; 0: the CTA-wide form (xtma_pass) with staged output copies.
+// Form of the contiguous passes at M = 128 and 256: 0 (default) the CTA-wide
+// form storing its outputs from registers; 1 the CTA-wide form with staged
+// output copies (tensor stores, or bulk row stores); 2 the warp-local form.
 int xpass_form();
 
 // Side modes of a pass: a 16-byte-aligned array moves by tensor boxes, rows
@@ -220,11 +224,15 @@ int launch_span_tensor_m128(int kind, const double* in, double* out, const PassA
                             const LineTables<double>& tb, int nv, cudaStream_t stream, const char* label);
 int launch_tensor_rows_m128(int kind, const double* in, double* out, const PassArgs& a,
                             const LineTables<double>& tb, int nv, cudaStream_t stream, const char* label);
+int launch_direct_m256(bool span, int kind, const double* in, double* out, const PassArgs& a,
+                       const LineTables<double>& tb, int nv, cudaStream_t stream, const char* label);
+int launch_direct_m128(bool span, int kind, const double* in, double* out, const PassArgs& a,
+                       const LineTables<double>& tb, int nv, cudaStream_t stream, const char* label);
 
 template <int M, int LDM, int STM>
 int launch_kinds(int kind, const double* in, double* out, const PassArgs& a, const LineTables<double>& tb, int nv,
                  cudaStream_t stream, const char* label) {
-    if constexpr (LDM == kLdTensor && STM == kStTensor) {
+    if constexpr (LDM == kLdTensor && (STM == kStTensor || STM == kStDirect)) {
         switch (kind) {
             case kDCT1: return launch_one<M, kDCT1, LDM, STM>(in, out, a, tb, nv, stream, label);
             case kDCT2: return launch_one<M, kDCT2, LDM, STM>(in, out, a, tb, nv, stream, label);
@@ -236,7 +244,7 @@ int launch_kinds(int kind, const double* in, double* out, const PassArgs& a, con
             case kC2R: return launch_one<M, kC2R, LDM, STM>(in, out, a, tb, nv, stream, label);
             default: return -1;
         }
-    } else if constexpr (LDM == kLdSpan && STM == kStTensor) {
+    } else if constexpr (LDM == kLdSpan && (STM == kStTensor || STM == kStDirect)) {
         switch (kind) {
             case kR2C: return launch_one<M, kR2C, LDM, STM>(in, out, a, tb, nv, stream, label);
             case kDST1: return launch_one<M, kDST1, LDM, STM>(in, out, a, tb, nv, stream, label);
@@ -268,7 +276,13 @@ int launch_xtma_kind(int kind, int kind2, const void* in, void* out, const PassA
     const double* pi = static_cast<const double*>(in);
     double* po = static_cast<double*>(out);
     const bool ld_tensor = rows_aligned(in, a.in_su, a.in_sv);
-    if (xpass_form() == 1) {
+    const int form = xpass_form();
+    if (form == 0 && (ld_tensor || span_side(in, a.in_su))) {
+        const int rc = (M == 256 ? launch_direct_m256 : launch_direct_m128)(!ld_tensor, kind, pi, po, a, tb, nv,
+                                                                            stream, label);
+        if (rc != -1) return rc;
+    }
+    if (form == 2) {
         int rc = -1;
         if (ld_tensor) rc = (M == 256 ? launch_w_tensor_m256 : launch_w_tensor_m128)(kind, pi, po, a, tb, nv, stream,
                                                                                       label);

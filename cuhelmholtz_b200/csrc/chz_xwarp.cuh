@@ -107,29 +107,6 @@ struct XWSmem {
     static constexpr size_t total = abort + 16 + 1024;  // + alignment slack
 };
 
-// Output sink of one line: entry l goes to row[l] (scaled) when l lies in the
-// output window [lo, hi] and the line exists; an entry pair 2m, 2m + 1 is one
-// 16-byte store when the row is 16-byte aligned.
-template <typename T>
-struct GSink {
-    T* row;
-    int lo, hi;
-    T sc;
-    bool al, on;
-    __device__ __forceinline__ void put(int l, T v) const {
-        if (on && l >= lo && l <= hi) row[l] = v * sc;
-    }
-    __device__ __forceinline__ void put2(int l, T x, T y) const {   // l even
-        if (on && al && l >= lo && l + 1 <= hi) {
-            *reinterpret_cast<C2<T>*>(row + l) = mk<T>(x * sc, y * sc);
-        } else {
-            put(l, x);
-            put(l + 1, y);
-        }
-    }
-    __device__ __forceinline__ void put_pair(int l, T x, T y) const { put2(l, x, y); }
-};
-
 // One real transform of one line by its P lanes: the real input is read
 // through X, the line's storage is then reused through Z for the exchanges,
 // and the outputs go to `sink` as they are formed.  The same pre steps,

@@ -1,10 +1,12 @@
 """GPU parity of the solver's x passes at N = 256 and 512, where the pipelined
 contiguous kernel moves the right-hand side f (rows of N + 1 values, 8-byte
-aligned) as one bulk span per tile.  Both forms of that kernel are run: the
-warp-local form (default: each line transformed by the lanes of one warp,
-results stored from registers inside the output window) and the CTA-wide
-form (the solution rows stored back with bulk copies of their 16-byte-aligned
-interiors plus plain stores of the ends).
+aligned) as one bulk span per tile.  The three forms of that kernel are run:
+the default (the 16 lines of a tile transformed together by the CTA, each
+thread storing its output entries from registers, inside the output window),
+the staged form (outputs staged in shared memory; the solution rows stored
+back with bulk copies of their 16-byte-aligned interiors plus plain stores of
+the ends) and the warp-local form (each line transformed by the lanes of one
+warp).
 
 Every x boundary code (its forward and inverse kinds), partial tiles (row
 counts that are not multiples of the 16-line tile), and f at both 16-byte
@@ -47,7 +49,7 @@ def _oracle(p):
                             p["f"])
 
 
-@pytest.fixture(params=["default", "cta_xpass"])
+@pytest.fixture(params=["default", "staged_xpass", "warp_xpass"])
 def xform(request):
     prev = api.set_kernel_family(request.param)
     yield request.param
@@ -76,13 +78,14 @@ def test_x_pass_512_many_tiles(xform):
     assert err < TOL, err
 
 
+@pytest.mark.parametrize("form", ["staged_xpass", "warp_xpass"])
 @pytest.mark.parametrize("n", [256, 512])
-def test_x_pass_forms_agree(n):
-    """The warp-local and CTA-wide forms give the same solve to round-off,
-    on a grid with many tiles per CTA, partial tiles and every boundary term."""
+def test_x_pass_forms_agree(n, form):
+    """The three forms give the same solve to round-off, on a grid with many
+    tiles per CTA, partial tiles and every boundary term."""
     p = gen.random_problem(n, 36, 90, 3, 1, 4, -0.8, seed=660 + n)
     a = _solve(p, 0)
-    prev = api.set_kernel_family("cta_xpass")
+    prev = api.set_kernel_family(form)
     try:
         b = _solve(p, 0)
     finally:
