@@ -816,7 +816,7 @@ def main():
     ap.add_argument("--refine-corrections", type=int, default=2,
                     help="also time the FP32 + FP64-refinement solve with this many corrections (-1: skip)")
     ap.add_argument("--kernel-family", default="default",
-                    choices=["default", "generic", "no_tma", "staged_xpass", "warp_xpass"],
+                    choices=["default", "generic", "no_tma"],
                     help="kernel family of the solver's passes (cuhelmholtz_b200.api.set_kernel_family)")
     args = ap.parse_args()
     args.sub_workloads = [w for w in args.sub_workloads.split(",") if w]

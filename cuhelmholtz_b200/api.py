@@ -291,16 +291,14 @@ class BatchPlan:
             pass
 
 
-KERNEL_FAMILIES = {"default": 0, "generic": 1, "no_tma": 2, "staged_xpass": 3, "warp_xpass": 4}
+KERNEL_FAMILIES = {"default": 0, "generic": 1, "no_tma": 2}
 
 
 def set_kernel_family(family) -> int:
-    """Selects the kernels: "default" (0: TMA-pipelined strided and
-    contiguous passes, register-resident line kernels, mixed-radix
-    elsewhere), "generic" (1, or True: the mixed-radix kernel for every pass),
-    "no_tma" (2), "staged_xpass" (3: the contiguous TMA pass staging its
-    outputs for store copies) or "warp_xpass" (4: its warp-local form).
-    Returns the previous setting (an int, accepted back)."""
+    """Selects the kernels: "default" (0: TMA-pipelined strided passes,
+    register-resident line kernels, mixed-radix elsewhere), "generic" (1, or
+    True: the mixed-radix kernel for every pass) or "no_tma" (2).  Returns the
+    previous setting (an int, accepted back)."""
     if isinstance(family, str):
         family = KERNEL_FAMILIES[family]
     elif isinstance(family, bool):

@@ -19,8 +19,6 @@
 // the complex FFT view and the real output view; phases are separated by
 // barriers.
 #pragma once
-#include <type_traits>
-
 #include "chz_device.cuh"
 #include "chz_internal.h"
 
@@ -226,32 +224,16 @@ struct OutSink {
     __device__ static __forceinline__ double recip(double d) { return recip_nr(d); }
 };
 
-// A sink whose outputs go to global memory (S::kGlobal) never writes the
-// tile buffer, so the transform writes each output as soon as it is formed
-// and skips the barriers that only order buffer writes after other threads'
-// reads.
-template <class S, class = void>
-struct GlobalSink {
-    static constexpr bool value = false;
-};
-template <class S>
-struct GlobalSink<S, std::void_t<decltype(S::kGlobal)>> {
-    static constexpr bool value = S::kGlobal;
-};
-
 // One complete real transform of the W lines held in `buf`: the real input of
 // line c is read through the view X (entry l: X(l)), the complex exchange view
 // Z[m * W + c] reuses `buf` once every input is in registers, and the real
-// output goes to `sink`.  With a global sink the transform ends without a
-// barrier: a caller that transforms another tile next must pass a `red` of
-// the other parity (the DCT-I partial sums are read in the post step).
+// output goes to `sink`.
 template <typename T, typename CF, int KIND, typename V, typename SINK>
 __device__ __forceinline__ void transform_lines_v(const V& X, T* buf, T* red, int c, int slot,
                                                   const LineTables<T>& tb, const SINK& sink) {
     constexpr int M = CF::M;
     constexpr int W = CF::W, N = CF::N, P = CF::P;
     constexpr bool FWD = (KIND == kR2C || KIND == kDCT2 || KIND == kDST2);
-    constexpr bool GS = GlobalSink<SINK>::value;
     C2<T>* Z = reinterpret_cast<C2<T>*>(buf);
     C2<T> v[kR];
 
@@ -310,26 +292,6 @@ __device__ __forceinline__ void transform_lines_v(const V& X, T* buf, T* red, in
     if constexpr (FWD) {
         // split: V[m] = 1/2 (Z[m] + conj Z[M-m]) - i/2 w^m (Z[m] - conj Z[M-m])
         C2<T> vM = mk<T>(T(0), T(0));
-        auto emit = [&](int m, const C2<T>& V) {
-            if constexpr (KIND == kR2C) {
-                sink.put_pair(2 * m, V.x, m == 0 ? T(0) : V.y);
-                if (m == 0) sink.put_pair(N, vM.x, T(0));
-            } else {
-                const C2<T> a = cmul<T>(ldtw<T>(tb.tw4N + m), V);
-                if constexpr (KIND == kDCT2) {
-                    sink.put(m, a.x);
-                    if (m > 0) sink.put(N - m, -a.y);
-                } else {  // DST2
-                    sink.put(N - m, a.x);
-                    if (m > 0) sink.put(m, -a.y);
-                    else sink.put(0, T(0));
-                }
-                if (m == 0) {
-                    const C2<T> aM = cmul<T>(ldtw<T>(tb.tw4N + M), vM);
-                    sink.put(M, aM.x);
-                }
-            }
-        };
 #pragma unroll
         for (int b = 0; b < LB::B; ++b)
 #pragma unroll
@@ -342,15 +304,33 @@ __device__ __forceinline__ void transform_lines_v(const V& X, T* buf, T* red, in
                 const C2<T> o = cmul<T>(wk, csub<T>(zk, cconj<T>(zm)));
                 v[b * LB::r + k] = mk<T>(T(0.5) * (e.x + o.y), T(0.5) * (e.y - o.x));
                 if (m == 0) vM = mk<T>(zk.x - zk.y, T(0));
-                if constexpr (GS) emit(m, v[b * LB::r + k]);
             }
-        if constexpr (!GS) {
-            CF::sync();
+        CF::sync();
 #pragma unroll
-            for (int b = 0; b < LB::B; ++b)
+        for (int b = 0; b < LB::B; ++b)
 #pragma unroll
-                for (int k = 0; k < LB::r; ++k) emit(LB::out_idx(slot, b, k), v[b * LB::r + k]);
-        }
+            for (int k = 0; k < LB::r; ++k) {
+                const int m = LB::out_idx(slot, b, k);
+                const C2<T> V = v[b * LB::r + k];
+                if constexpr (KIND == kR2C) {
+                    sink.put_pair(2 * m, V.x, m == 0 ? T(0) : V.y);
+                    if (m == 0) sink.put_pair(N, vM.x, T(0));
+                } else {
+                    const C2<T> a = cmul<T>(ldtw<T>(tb.tw4N + m), V);
+                    if constexpr (KIND == kDCT2) {
+                        sink.put(m, a.x);
+                        if (m > 0) sink.put(N - m, -a.y);
+                    } else {  // DST2
+                        sink.put(N - m, a.x);
+                        if (m > 0) sink.put(m, -a.y);
+                        else sink.put(0, T(0));
+                    }
+                    if (m == 0) {
+                        const C2<T> aM = cmul<T>(ldtw<T>(tb.tw4N + M), vM);
+                        sink.put(M, aM.x);
+                    }
+                }
+            }
     } else if constexpr (KIND == kDCT1 || KIND == kDST1) {
         // v[n] = Re conj(Z[n/2]) (n even), Im conj(Z[n/2]) (n odd); pairs (k, N-k)
         T outs[2 * kR];
@@ -390,29 +370,20 @@ __device__ __forceinline__ void transform_lines_v(const V& X, T* buf, T* red, in
                 T oo;
                 if constexpr (KIND == kDCT1) oo = ((vo + po) * T(0.5) - (vo - po) * is4o) * T(0.5);
                 else oo = ((vo + po) * is4o + (vo - po) * T(0.5)) * T(0.5);
-                if constexpr (GS) {
-                    sink.put2(2 * m, oe, oo);
-                    if constexpr (KIND == kDCT1) {
-                        if (m == 0) sink.put(N, extra);
-                    }
-                } else {
-                    outs[2 * (b * LB::r + k)] = oe;
-                    outs[2 * (b * LB::r + k) + 1] = oo;
+                outs[2 * (b * LB::r + k)] = oe;
+                outs[2 * (b * LB::r + k) + 1] = oo;
+            }
+        CF::sync();
+#pragma unroll
+        for (int b = 0; b < LB::B; ++b)
+#pragma unroll
+            for (int k = 0; k < LB::r; ++k) {
+                const int m = LB::out_idx(slot, b, k);
+                sink.put2(2 * m, outs[2 * (b * LB::r + k)], outs[2 * (b * LB::r + k) + 1]);
+                if constexpr (KIND == kDCT1) {
+                    if (m == 0) sink.put(N, extra);
                 }
             }
-        if constexpr (!GS) {
-            CF::sync();
-#pragma unroll
-            for (int b = 0; b < LB::B; ++b)
-#pragma unroll
-                for (int k = 0; k < LB::r; ++k) {
-                    const int m = LB::out_idx(slot, b, k);
-                    sink.put2(2 * m, outs[2 * (b * LB::r + k)], outs[2 * (b * LB::r + k) + 1]);
-                    if constexpr (KIND == kDCT1) {
-                        if (m == 0) sink.put(N, extra);
-                    }
-                }
-        }
     } else {
         // C2R, DCT3, DST3: outputs come straight from the thread's own values
         // (every thread passed the barrier after its last shared reads)
@@ -438,7 +409,7 @@ __device__ __forceinline__ void transform_lines_v(const V& X, T* buf, T* red, in
                 }
             }
     }
-    if constexpr (!GS) CF::sync();
+    CF::sync();
 }
 
 // The same with the configuration's own real view of `buf`.

@@ -78,13 +78,6 @@ __global__ void periodic_fixup(double* f, int nx, int ny, int nz, int px, int py
 
 std::atomic<int> g_force_generic{0};
 
-namespace xtma {
-int xpass_form() {
-    const int f = g_force_generic.load(std::memory_order_relaxed);
-    return f == 3 ? 1 : (f == 4 ? 2 : 0);
-}
-}  // namespace xtma
-
 int factor_radices(int M, RadixPlan* rp) {
     int m = M;
     int e2 = 0;
@@ -359,11 +352,11 @@ int launch_line_pass(int is_double, int in_type, int out_type, bool contig, cons
                      void* out, const PassArgs& a, const DeviceLineTables& tb, const LineGeom& g,
                      int nv, cudaStream_t stream, const char* label) {
     const int family = g_force_generic.load(std::memory_order_relaxed);
-    if (contig && (family == 0 || family >= 3) && is_double && in_type == kIoF64 && out_type == kIoF64) {
+    if (contig && family == 0 && is_double && in_type == kIoF64 && out_type == kIoF64) {
         const int rc = try_xtma(in, out, a, tb, nv, stream, label);
         if (rc != -1) return rc;
     }
-    if (!contig && (family == 0 || family >= 3) && in_type == out_type) {
+    if (!contig && family == 0 && in_type == out_type) {
         const int rc = is_double ? try_tma<double>(in, out, a, tb, nv, stream, label)
                                  : try_tma<float>(in, out, a, tb, nv, stream, label);
         if (rc != -1) return rc;
@@ -511,11 +504,11 @@ int chz_trace_collect(char* buf, size_t len) {
     return n;
 }
 
-// Selects the kernel family (0 default, 1 generic, 2 no TMA kernels, 3 the
-// contiguous TMA pass with staged output copies, 4 its warp-local form);
-// returns the previous setting.
+// Selects the kernel family: 0 = register-resident kernels where supported
+// (default), 1 = the generic shared-memory kernel for every length.  Returns
+// the previous setting.
 int chz_set_kernel_family(int family) {
-    if (family < 0 || family > 4) return -1;
+    if (family < 0 || family > 2) return -1;
     return g_force_generic.exchange(family);
 }
 

@@ -93,32 +93,6 @@ struct SwzSink {
     __device__ __forceinline__ void put2(int l, T a, T b) const { put_pair(l, a, b); }
 };
 
-// Output sink of one line in global memory: entry l goes to row[l] (scaled)
-// when l lies in the output window [lo, hi] and the line exists; an entry pair
-// 2m, 2m + 1 is one 16-byte store when `al` (the caller sets it only where the
-// row is 16-byte aligned; a flag shared by all lines of a pass keeps the lanes
-// of a warp on one path).
-template <typename T>
-struct GSink {
-    static constexpr bool kGlobal = true;
-    T* row;
-    int lo, hi;
-    T sc;
-    bool al, on;
-    __device__ __forceinline__ void put(int l, T v) const {
-        if (on && l >= lo && l <= hi) row[l] = v * sc;
-    }
-    __device__ __forceinline__ void put2(int l, T x, T y) const {   // l even
-        if (on && al && l >= lo && l + 1 <= hi) {
-            *reinterpret_cast<C2<T>*>(row + l) = mk<T>(x * sc, y * sc);
-        } else {
-            put(l, x);
-            put(l + 1, y);
-        }
-    }
-    __device__ __forceinline__ void put_pair(int l, T x, T y) const { put2(l, x, y); }
-};
-
 struct XGeom {
     int ld_blk0, ld_nblk;   // tensor-loaded blocks (LD_TMA)
     int st_blk0, st_nblk;   // tensor-stored blocks (ST_TMA)
@@ -134,9 +108,7 @@ struct XSmem {
     static constexpr size_t tw4N = twN + sizeof(C2<T>) * (M + 1);
     static constexpr size_t inv4sin = tw4N + sizeof(C2<T>) * (M + 1);
     static constexpr size_t red = (inv4sin + sizeof(T) * (M + 1) + 15) & ~size_t(15);
-    // two sets of DCT-I partial sums (tiles alternate; the direct-store form
-    // ends a tile without a barrier)
-    static constexpr size_t bars = (red + 2 * sizeof(T) * CF::RED + 15) & ~size_t(15);
+    static constexpr size_t bars = (red + sizeof(T) * CF::RED + 15) & ~size_t(15);
     static constexpr size_t abort = bars + 2 * kStages * sizeof(uint64_t);
     static constexpr size_t total = abort + 16 + 1024;  // + alignment slack
 };
@@ -145,12 +117,9 @@ __device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* b) {
     asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(saddr(b)) : "memory");
 }
 
-// How each side of a tile moves.  kStDirect: no store copy -- each compute
-// thread writes its output entries from registers straight to global memory
-// (inside the output window; entry pairs as 16-byte stores when every row is
-// 16-byte aligned).
+// How each side of a tile moves.
 enum XLoad { kLdTensor = 0, kLdSpan = 1 };
-enum XStore { kStTensor = 0, kStRows = 1, kStDirect = 2 };
+enum XStore { kStTensor = 0, kStRows = 1 };
 
 // Row-major real view of one line (span loads): entry l at line[l].
 template <typename T>
@@ -303,15 +272,6 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
         for (int i = 0; i < pre; ++i) issue_load(i);
         for (int i = 0; i < nloc; ++i) {
             const int s = i % kStages;
-            if constexpr (STM == kStDirect) {
-                // the compute threads stored the tile themselves: the stage is
-                // refilled as soon as they have read it
-                if (i + kStages >= nloc) continue;
-                if (!mbar_wait(ready + s, (uint32_t)((i / kStages) & 1), abort, wait_limit))
-                    atomicOr(flags, kFlagProducer);
-                issue_load(i + kStages);
-                continue;
-            }
             if (!mbar_wait(ready + s, (uint32_t)((i / kStages) & 1), abort, wait_limit))
                 atomicOr(flags, kFlagProducer);
             int ub, v, nl;
@@ -344,7 +304,7 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
                 issue_load(i + kStages);
             }
         }
-        if constexpr (STM != kStDirect) asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+        asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
         tma::drain_loads(full, nloc, kStages, wait_limit, flags);
         return;
     }
@@ -353,9 +313,6 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
     const int c = t % W;
     const int slot = t / W;
     const double sc = a.use_scale ? a.scale : 1.0;
-    // direct stores: entry pairs as 16-byte stores only when every output row
-    // of the pass starts on a 16-byte boundary
-    const bool al_out = !(reinterpret_cast<uintptr_t>(out) & 15) && !(a.out_su & 1) && !(a.out_sv & 1);
     // The boundary terms at xs and xe of a tile's rows off the y and z
     // boundaries (one (row, side) per thread) are one global value each (a
     // face entry of f or a Neumann array) times a coefficient: the value of
@@ -448,13 +405,9 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
             if constexpr (STM == kStTensor) {
                 SwzSink<T> sink{buf, c};
                 transform_lines_v<T, CF, KIND>(X, buf, red, c, slot, tb, sink);
-            } else if constexpr (STM == kStRows) {
+            } else {
                 RowSink<T> sink{buf + offo + c * (int)a.out_su, sc};
                 transform_lines_v<T, CF, KIND>(X, buf, red, c, slot, tb, sink);
-            } else {
-                const GSink<T> sink{out_row0(ub, v) + (long long)c * a.out_su, a.st_lo, a.st_hi, (T)sc, al_out,
-                                    c < nl};
-                transform_lines_v<T, CF, KIND>(X, buf, red + (i & 1) * CF::RED, c, slot, tb, sink);
             }
         };
         if constexpr (LDM == kLdSpan) run(RowView<T>{buf + off + c * (int)a.in_su});
@@ -476,7 +429,7 @@ xtma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUt
             }
         }
         // make this thread's writes visible to the bulk / tensor stores, then release
-        if constexpr (STM != kStDirect) asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         mbar_arrive(ready + s);
     }
 }

@@ -8,7 +8,7 @@
 #include <atomic>
 #include <cstdint>
 
-#include "chz_xwarp.cuh"
+#include "chz_xtma.cuh"
 
 namespace chz {
 namespace fast {
@@ -60,10 +60,7 @@ int launch_one(const double* in, double* out, const PassArgs& a, const LineTable
         // row, and the W rows (plus the span's misalignment) inside a stage
         if (HI > a.in_su - 1 || a.in_sv < a.in_su * (a.u0 + a.nu) || W * a.in_su + 2 > CF::BUF) return -1;
     }
-    if (STM == kStDirect) {
-        // the output window inside a row, 8-byte-aligned rows
-        if (a.st_lo < 0 || a.st_hi > a.out_su - 1 || (reinterpret_cast<uintptr_t>(out) & 7)) return -1;
-    } else if (STM == kStTensor) {
+    if (STM == kStTensor) {
         g.st_blk0 = a.st_lo >> 4;
         g.st_nblk = (a.st_hi >> 4) - g.st_blk0 + 1;
         const unsigned long long dims[3] = {(unsigned long long)(a.st_hi + 1), (unsigned long long)(a.u0 + a.nu),
@@ -108,105 +105,6 @@ int launch_one(const double* in, double* out, const PassArgs& a, const LineTable
     return (int)cudaGetLastError();
 }
 
-// Launches one instantiation of the warp-local form; -1 when the geometry
-// does not fit it.
-template <int M, int KIND, int LDM>
-int launch_w(const double* in, double* out, const PassArgs& a, const LineTables<double>& tb, int nv,
-             cudaStream_t stream, const char* label) {
-    using CF = XCfg<M>;
-    using SL = XWSmem<double, M>;
-    constexpr int W = CF::W, N = CF::N;
-    constexpr int LO = fast::InWin<KIND, N>::lo, HI = fast::InWin<KIND, N>::hi;
-    if ((long long)SL::total > (long long)tma::max_optin_smem()) return -1;
-    if (LDM == kLdTensor && a.has_bc) return -1;   // boundary terms come with a span input only
-    XGeom g{};
-    CUtensorMap ldmap;
-    std::memset(&ldmap, 0, sizeof(ldmap));
-    g.v_off = a.v0;
-    if (LDM == kLdTensor) {
-        g.ld_blk0 = LO >> 4;
-        g.ld_nblk = (HI >> 4) - g.ld_blk0 + 1;
-        const unsigned box[3] = {16u, 16u, 1u};
-        const unsigned long long dims[3] = {(unsigned long long)(a.ld_hi + 1), (unsigned long long)(a.u0 + a.nu),
-                                            (unsigned long long)nv};
-        const unsigned long long strides[2] = {(unsigned long long)(a.in_su * 8), (unsigned long long)(a.in_sv * 8)};
-        if (!tma::encode_map_swz(&ldmap, in + (long long)a.v0 * a.in_sv, dims, strides, box)) return -1;
-    } else {
-        // whole rows of the span, row-major: the kind's input window inside a
-        // row, 2M + 1 entries a row (the exchange view of a line stays in its
-        // row), and the W rows (plus the span's misalignment) inside a stage
-        if (HI > a.in_su - 1 || a.in_su < N + 1 || a.in_sv < a.in_su * (a.u0 + a.nu) || W * a.in_su + 2 > CF::BUF)
-            return -1;
-    }
-    // the output window inside a row, 8-byte-aligned rows
-    if (a.st_lo < 0 || a.st_hi > a.out_su - 1 || (reinterpret_cast<uintptr_t>(out) & 7)) return -1;
-    int* flags = tma::device_flags();
-    if (!flags) return -1;
-    auto kern = xw_pass<double, M, KIND, LDM>;
-    constexpr int threads = CF::NT;
-    static std::atomic<int> cps_cached{0};
-    int cps = cps_cached.load(std::memory_order_relaxed);
-    if (cps == 0) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SL::total);
-        if (e != cudaSuccess) return (int)e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cps, kern, threads, SL::total);
-        if (e != cudaSuccess) return (int)e;
-        if (cps < 1) return -1;
-        cps_cached.store(cps, std::memory_order_relaxed);
-    }
-    const int ntx = (a.nu + W - 1) / W;
-    const long long ntiles = (long long)ntx * nv;
-    if (ntiles <= 0) return 0;
-    if (ntiles > 0x7fffffffLL) return -1;
-    const long long cap = (long long)cps * fast::device_sm_count();
-    const int grid = (int)std::min(ntiles, cap);
-    trace_begin(stream, label);
-    kern<<<grid, threads, SL::total, stream>>>(ldmap, in, out, a, tb, g, ntx, (int)ntiles, flags,
-                                                tma::wait_limit());
-    count_launch();
-    trace_end(stream);
-    return (int)cudaGetLastError();
-}
-
-// Every kind of the warp-local form with a tensor input (do_transform, the
-// solver's inverse passes from the work array), and the solver's forward
-// kinds with a span input (f).
-template <int M, int LDM>
-int launch_w_kinds(int kind, const double* in, double* out, const PassArgs& a, const LineTables<double>& tb, int nv,
-                   cudaStream_t stream, const char* label) {
-    switch (kind) {
-        case kDCT1: return launch_w<M, kDCT1, LDM>(in, out, a, tb, nv, stream, label);
-        case kDCT3: return launch_w<M, kDCT3, LDM>(in, out, a, tb, nv, stream, label);
-        case kDST1: return launch_w<M, kDST1, LDM>(in, out, a, tb, nv, stream, label);
-        case kDST3: return launch_w<M, kDST3, LDM>(in, out, a, tb, nv, stream, label);
-        case kR2C: return launch_w<M, kR2C, LDM>(in, out, a, tb, nv, stream, label);
-        default: break;
-    }
-    if constexpr (LDM == kLdTensor) {
-        switch (kind) {
-            case kDCT2: return launch_w<M, kDCT2, LDM>(in, out, a, tb, nv, stream, label);
-            case kDST2: return launch_w<M, kDST2, LDM>(in, out, a, tb, nv, stream, label);
-            case kC2R: return launch_w<M, kC2R, LDM>(in, out, a, tb, nv, stream, label);
-            default: break;
-        }
-    }
-    return -1;
-}
-
-int launch_w_tensor_m256(int kind, const double* in, double* out, const PassArgs& a, const LineTables<double>& tb,
-                         int nv, cudaStream_t stream, const char* label);
-int launch_w_span_m256(int kind, const double* in, double* out, const PassArgs& a, const LineTables<double>& tb,
-                       int nv, cudaStream_t stream, const char* label);
-int launch_w_tensor_m128(int kind, const double* in, double* out, const PassArgs& a, const LineTables<double>& tb,
-                         int nv, cudaStream_t stream, const char* label);
-int launch_w_span_m128(int kind, const double* in, double* out, const PassArgs& a, const LineTables<double>& tb,
-                       int nv, cudaStream_t stream, const char* label);
-
-// Form of the contiguous passes at M = 128 and 256: 0 (default) the CTA-wide
-// form storing its outputs from registers; 1 the CTA-wide form with staged
-// output copies (tensor stores, or bulk row stores); 2 the warp-local form.
-int xpass_form();
-
 // Side modes of a pass: a 16-byte-aligned array moves by tensor boxes, rows
 // of an 8-byte-aligned array (the solver's f) by bulk copies of the span.
 inline bool span_side(const void* p, long long pitch) {
@@ -224,15 +122,11 @@ int launch_span_tensor_m128(int kind, const double* in, double* out, const PassA
                             const LineTables<double>& tb, int nv, cudaStream_t stream, const char* label);
 int launch_tensor_rows_m128(int kind, const double* in, double* out, const PassArgs& a,
                             const LineTables<double>& tb, int nv, cudaStream_t stream, const char* label);
-int launch_direct_m256(bool span, int kind, const double* in, double* out, const PassArgs& a,
-                       const LineTables<double>& tb, int nv, cudaStream_t stream, const char* label);
-int launch_direct_m128(bool span, int kind, const double* in, double* out, const PassArgs& a,
-                       const LineTables<double>& tb, int nv, cudaStream_t stream, const char* label);
 
 template <int M, int LDM, int STM>
 int launch_kinds(int kind, const double* in, double* out, const PassArgs& a, const LineTables<double>& tb, int nv,
                  cudaStream_t stream, const char* label) {
-    if constexpr (LDM == kLdTensor && (STM == kStTensor || STM == kStDirect)) {
+    if constexpr (LDM == kLdTensor && STM == kStTensor) {
         switch (kind) {
             case kDCT1: return launch_one<M, kDCT1, LDM, STM>(in, out, a, tb, nv, stream, label);
             case kDCT2: return launch_one<M, kDCT2, LDM, STM>(in, out, a, tb, nv, stream, label);
@@ -244,7 +138,7 @@ int launch_kinds(int kind, const double* in, double* out, const PassArgs& a, con
             case kC2R: return launch_one<M, kC2R, LDM, STM>(in, out, a, tb, nv, stream, label);
             default: return -1;
         }
-    } else if constexpr (LDM == kLdSpan && (STM == kStTensor || STM == kStDirect)) {
+    } else if constexpr (LDM == kLdSpan && STM == kStTensor) {
         switch (kind) {
             case kR2C: return launch_one<M, kR2C, LDM, STM>(in, out, a, tb, nv, stream, label);
             case kDST1: return launch_one<M, kDST1, LDM, STM>(in, out, a, tb, nv, stream, label);
@@ -276,20 +170,6 @@ int launch_xtma_kind(int kind, int kind2, const void* in, void* out, const PassA
     const double* pi = static_cast<const double*>(in);
     double* po = static_cast<double*>(out);
     const bool ld_tensor = rows_aligned(in, a.in_su, a.in_sv);
-    const int form = xpass_form();
-    if (form == 0 && (ld_tensor || span_side(in, a.in_su))) {
-        const int rc = (M == 256 ? launch_direct_m256 : launch_direct_m128)(!ld_tensor, kind, pi, po, a, tb, nv,
-                                                                            stream, label);
-        if (rc != -1) return rc;
-    }
-    if (form == 2) {
-        int rc = -1;
-        if (ld_tensor) rc = (M == 256 ? launch_w_tensor_m256 : launch_w_tensor_m128)(kind, pi, po, a, tb, nv, stream,
-                                                                                      label);
-        else if (span_side(in, a.in_su))
-            rc = (M == 256 ? launch_w_span_m256 : launch_w_span_m128)(kind, pi, po, a, tb, nv, stream, label);
-        if (rc != -1) return rc;
-    }
     const bool st_tensor = rows_aligned(out, a.out_su, a.out_sv) && !a.use_scale;
     if (ld_tensor && st_tensor) return launch_kinds<M, kLdTensor, kStTensor>(kind, pi, po, a, tb, nv, stream, label);
     auto span = M == 256 ? launch_span_tensor_m256 : launch_span_tensor_m128;

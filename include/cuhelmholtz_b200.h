@@ -303,17 +303,13 @@ int chz_release_cached(void);
 int chz_trace_enable(int on);
 int chz_trace_collect(char* buf, size_t len);
 
-/* Kernel family: 0 (default) uses the TMA-pipelined kernels for the strided
- * (y, z) passes of N = 128, 256, 512 and for the contiguous (x) passes of
- * N = 256, 512 (which store their outputs from registers), the
- * register-resident line kernels for the other passes of lengths N = 32..1024
- * that are powers of two, and the shared-memory mixed-radix kernel elsewhere;
- * 1 uses the mixed-radix kernel for every pass; 2 is family 0 without the TMA
- * kernels; 3 is family 0 with the contiguous TMA pass staging its outputs in
- * shared memory for tensor / bulk store copies; 4 is family 0 with the
- * warp-local form of the contiguous TMA pass (each line transformed by the
- * lanes of one warp).  All are checked against the same oracle.  Returns the
- * previous setting, or -1 for an unknown family. */
+/* Kernel family: 0 (default) uses the TMA-pipelined kernel for the strided
+ * (y, z) passes of N = 128, 256, 512, the register-resident line kernels for
+ * the other passes of lengths N = 32..1024 that are powers of two, and the
+ * shared-memory mixed-radix kernel elsewhere; 1 uses the mixed-radix kernel
+ * for every pass; 2 is family 0 without the TMA kernel (all are checked
+ * against the same oracle).  Returns the previous setting, or -1 for an
+ * unknown family. */
 int chz_set_kernel_family(int family);
 
 /* Flags raised by the kernels' bounded waits since the last reset (0 when no

@@ -117,7 +117,7 @@ def test_config3_512_manufactured_exact():
     assert err < TOL, err
 
 
-@pytest.mark.parametrize("family", ["generic", "no_tma", "staged_xpass", "warp_xpass"])
+@pytest.mark.parametrize("family", ["generic", "no_tma"])
 @pytest.mark.parametrize("bcs", [(1, 2, 0), (3, 4, 0), (0, 0, 0), (2, 1, 4), (4, 3, 2), (1, 1, 1), (3, 3, 3)])
 def test_kernel_families_agree(bcs, family):
     """The TMA-pipelined, register-resident and generic kernels give the same

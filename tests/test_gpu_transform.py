@@ -53,7 +53,7 @@ def test_all_kind_triples_small(inplace, dims):
         _check(d, nx, ny, nz, kinds, inplace)
 
 
-@pytest.fixture(params=["default", "generic", "no_tma", "staged_xpass", "warp_xpass"])
+@pytest.fixture(params=["default", "generic", "no_tma"])
 def kernel_family(request):
     prev = api.set_kernel_family(request.param)
     yield request.param

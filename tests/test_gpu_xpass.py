@@ -1,12 +1,7 @@
 """GPU parity of the solver's x passes at N = 256 and 512, where the pipelined
 contiguous kernel moves the right-hand side f (rows of N + 1 values, 8-byte
-aligned) as one bulk span per tile.  The three forms of that kernel are run:
-the default (the 16 lines of a tile transformed together by the CTA, each
-thread storing its output entries from registers, inside the output window),
-the staged form (outputs staged in shared memory; the solution rows stored
-back with bulk copies of their 16-byte-aligned interiors plus plain stores of
-the ends) and the warp-local form (each line transformed by the lanes of one
-warp).
+aligned) as one bulk span per tile and stores the solution rows back with
+bulk copies of their 16-byte-aligned interiors plus plain stores of the ends.
 
 Every x boundary code (its forward and inverse kinds), partial tiles (row
 counts that are not multiples of the 16-line tile), and f at both 16-byte
@@ -49,17 +44,10 @@ def _oracle(p):
                             p["f"])
 
 
-@pytest.fixture(params=["default", "staged_xpass", "warp_xpass"])
-def xform(request):
-    prev = api.set_kernel_family(request.param)
-    yield request.param
-    api.set_kernel_family(prev)
-
-
 @pytest.mark.parametrize("n", [256, 512])
 @pytest.mark.parametrize("phase", [0, 1])
 @pytest.mark.parametrize("xbc,ybc,zbc", [(0, 1, 3), (1, 3, 0), (2, 4, 2), (3, 4, 0), (4, 0, 1)])
-def test_x_pass_every_code(xbc, ybc, zbc, phase, n, xform):
+def test_x_pass_every_code(xbc, ybc, zbc, phase, n):
     p = gen.random_problem(n, 12, 20, xbc, ybc, zbc, -3.0, seed=600 + 10 * xbc + phase + n)
     got = _solve(p, phase)
     ref = _oracle(p)
@@ -67,7 +55,7 @@ def test_x_pass_every_code(xbc, ybc, zbc, phase, n, xform):
     assert err < TOL, err
 
 
-def test_x_pass_512_many_tiles(xform):
+def test_x_pass_512_many_tiles():
     """Enough tiles for several per CTA (the three-stage pipeline wraps
     around: 4 tiles a plane x 160 planes over 148 CTAs) with a partial last
     tile in every plane (49 rows)."""
@@ -76,18 +64,3 @@ def test_x_pass_512_many_tiles(xform):
     ref = _oracle(p)
     err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
     assert err < TOL, err
-
-
-@pytest.mark.parametrize("form", ["staged_xpass", "warp_xpass"])
-@pytest.mark.parametrize("n", [256, 512])
-def test_x_pass_forms_agree(n, form):
-    """The three forms give the same solve to round-off, on a grid with many
-    tiles per CTA, partial tiles and every boundary term."""
-    p = gen.random_problem(n, 36, 90, 3, 1, 4, -0.8, seed=660 + n)
-    a = _solve(p, 0)
-    prev = api.set_kernel_family(form)
-    try:
-        b = _solve(p, 0)
-    finally:
-        api.set_kernel_family(prev)
-    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-13
