@@ -1,24 +1,28 @@
-// Register-resident line-pass kernel for power-of-two half lengths
-// M = N/2 in {16, 32, 64, 128, 256, 512} (N = 32 .. 1024).
+// Register-resident line-pass kernel for half lengths M = N/2 with a
+// compile-time radix plan: the powers of two 16 .. 512 (N = 32 .. 1024) and a
+// set of mixed lengths (M = 12 .. 192 with factors 3, 5, 7).
 //
-// * Each line is transformed by P = M/16 threads; every thread keeps 16
-//   complex values in registers and performs radix-16 butterflies (radix
-//   2/4/8 for the last factor) between shared-memory exchanges (Stockham
-//   order).  The kind's pre step is fused into the first stage's reads, the
-//   post step reads only the partner values each output needs, and in the
-//   fused solver pass the eigenvalue division is applied while the forward
-//   post step writes.
+// * Each line is transformed by P = M/V threads; every thread keeps V complex
+//   values in registers (V = 16 for the powers of two: radix-16 butterflies,
+//   radix 2/4/8 for the last factor; V = 10 .. 20 for the mixed lengths, whose
+//   radices -- 10, 12, 14, 18, 20 and 2, 4 -- are computed in registers as
+//   nested small DFTs) between shared-memory exchanges (Stockham order).  The
+//   kind's pre step is fused into the first stage's reads, the post step reads
+//   only the partner values each output needs, and in the fused solver pass
+//   the eigenvalue division is applied while the forward post step writes.
 // * The transform kind (and the inverse kind of a fused pass) are template
 //   parameters, so every index, window bound and branch is resolved at
 //   compile time.
 // * CTAs are persistent: each stages its line tables in shared memory once and
 //   loops over tiles of W lines; a tile is loaded with cp.async (every copy in
-//   flight at once) and four CTAs per SM overlap one another's loads, FFT work
-//   and stores.
+//   flight at once) and several CTAs per SM overlap one another's loads, FFT
+//   work and stores.
 // One tile buffer of (N+2) x (W+1) values holds, in turn, the real input view,
 // the complex FFT view and the real output view; phases are separated by
 // barriers.
 #pragma once
+#include <utility>
+
 #include "chz_device.cuh"
 #include "chz_internal.h"
 
@@ -26,25 +30,58 @@ namespace chz {
 namespace fast {
 
 constexpr int kNT = 128;  // threads per CTA
-constexpr int kR = 16;    // complex values per thread
+constexpr int kR = 16;    // complex values per thread of the power-of-two plans
 
-// Geometry of a tile of W lines transformed by P = M/16 threads each: the real
+// Radix plan of one half length M: V complex values per thread and the radix
+// of each Stockham stage (every radix divides V, their product is M).  Powers
+// of two: radix 16 stages, then the remaining factor 2, 4 or 8.
+template <int M>
+struct Plan {
+    static_assert(M >= 16 && (M & (M - 1)) == 0, "no radix plan for this length");
+    static constexpr int V = kR;
+    static constexpr int A16 = (M >= 256) ? 2 : 1;
+    static constexpr int R0 = M / (A16 == 2 ? 256 : 16);
+    static constexpr int NST = A16 + (R0 > 1 ? 1 : 0);
+    __host__ __device__ static constexpr int radix(int s) { return s < A16 ? 16 : R0; }
+};
+template <int V_, int R0_, int R1_ = 1, int R2_ = 1, int R3_ = 1>
+struct MixedPlan {
+    static constexpr int V = V_;
+    static constexpr int NST = 1 + (R1_ > 1) + (R2_ > 1) + (R3_ > 1);
+    __host__ __device__ static constexpr int radix(int s) {
+        return s == 0 ? R0_ : s == 1 ? R1_ : s == 2 ? R2_ : R3_;
+    }
+};
+// The mixed lengths: P = M / V threads a line divides the 128 threads of a CTA.
+template <> struct Plan<12> : MixedPlan<12, 12> {};
+template <> struct Plan<20> : MixedPlan<10, 10, 2> {};
+template <> struct Plan<24> : MixedPlan<12, 12, 2> {};
+template <> struct Plan<28> : MixedPlan<14, 14, 2> {};
+template <> struct Plan<40> : MixedPlan<10, 10, 2, 2> {};
+template <> struct Plan<48> : MixedPlan<12, 12, 4> {};
+template <> struct Plan<56> : MixedPlan<14, 14, 2, 2> {};
+template <> struct Plan<72> : MixedPlan<18, 18, 2, 2> {};
+template <> struct Plan<80> : MixedPlan<20, 20, 4> {};
+template <> struct Plan<96> : MixedPlan<12, 12, 4, 2> {};
+template <> struct Plan<160> : MixedPlan<20, 20, 4, 2> {};
+template <> struct Plan<192> : MixedPlan<12, 12, 4, 4> {};
+
+// Geometry of a tile of W lines transformed by P = M/V threads each: the real
 // view of entry l of line c is buf[l * PR + c], the complex view of entry m is
 // Z[m * W + c].  BAR = 0 synchronises the CTA with __syncthreads; BAR > 0 uses
 // named barrier BAR over the NT compute threads only.
 template <int M_, int W_, int PR_, int BAR_>
 struct LineCfg {
     static constexpr int M = M_;
-    static constexpr int P = M / kR;      // threads per line
+    static constexpr int V = Plan<M>::V;  // values per thread
+    static constexpr int P = M / V;       // threads per line
     static constexpr int W = W_;          // lines per tile
     static constexpr int NT = P * W;      // compute threads
     static constexpr int N = 2 * M;
     static constexpr int L = N + 2;       // padded line
     static constexpr int PR = PR_;        // real-view pitch
     static constexpr int BAR = BAR_;
-    static constexpr int A16 = (M >= 256) ? 2 : 1;               // radix-16 stages
-    static constexpr int R0 = M / (A16 == 2 ? 256 : 16);          // last radix (1 = none)
-    static constexpr int NST = A16 + (R0 > 1 ? 1 : 0);
+    static constexpr int NST = Plan<M>::NST;
     static constexpr int BUF = ((L * PR) + 3) & ~3;   // elements per tile buffer (>= 2*M*W)
     static constexpr int RED = P * W;      // DCT1 odd-sum partials
     __device__ static __forceinline__ void sync() {
@@ -62,7 +99,7 @@ struct LineCfg {
 // The persistent cp.async kernel: 128 threads, odd pitch W + 1 (conflict-free
 // transposed access).
 template <int M>
-using Cfg = LineCfg<M, kNT / (M / kR), kNT / (M / kR) + 1, 0>;
+using Cfg = LineCfg<M, kNT / (M / Plan<M>::V), kNT / (M / Plan<M>::V) + 1, 0>;
 
 #define CHZ_C1 0.92387953251128675613
 #define CHZ_S1 0.38268343236508977173
@@ -108,11 +145,92 @@ __device__ __forceinline__ void dft_r(C2<T>* v) {
     else if constexpr (r == 2) Dft<T, 2>::run(v, nullptr, 0);
 }
 
+// a * w_R^t (w_R = exp(-2 pi i / R)) with t a compile-time exponent: the
+// eighth roots of unity in closed form, every other factor from the M-point
+// table (w_R^t = twM[t M / R]; R divides M).
+template <typename T, int R, int t, int M>
+__device__ __forceinline__ C2<T> rot(C2<T> a, const C2<T>* __restrict__ twM) {
+    constexpr int u = t % R;
+    if constexpr (u == 0) return a;
+    else if constexpr (4 * u == R) return cmul_negi<T>(a);
+    else if constexpr (2 * u == R) return mk<T>(-a.x, -a.y);
+    else if constexpr (4 * u == 3 * R) return cmul_i<T>(a);
+    else if constexpr (8 * u == R) {
+        const T r = T(CHZ_SQRT_HALF);
+        return mk<T>(r * (a.x + a.y), r * (a.y - a.x));
+    } else if constexpr (8 * u == 3 * R) {
+        const T r = T(CHZ_SQRT_HALF);
+        return mk<T>(r * (a.y - a.x), -r * (a.x + a.y));
+    } else {
+        return cmul<T>(a, ldtw<T>(twM + u * (M / R)));
+    }
+}
+
+template <typename T, int R, int M>
+__device__ __forceinline__ void dft_plan(C2<T>* v, const C2<T>* __restrict__ twM);
+
+// Radix R = R1 R2 in registers (Cooley-Tukey): with n = R2 n1 + n2 and
+// k = k1 + R1 k2, X[k] = sum_n2 w_R2^(n2 k2) w_R^(n2 k1) sum_n1 w_R1^(n1 k1) v[n].
+// Column n2: the R1-point DFT of v[R2 n1 + n2], twiddled into a[k1 R2 + n2]
+// (the exponents n2 k1 are template arguments, so the trivial ones fold).
+template <typename T, int R1, int R2, int M, int n2, int... k1>
+__device__ __forceinline__ void ct_twiddle(const C2<T>* u, C2<T>* a, const C2<T>* __restrict__ twM,
+                                           std::integer_sequence<int, k1...>) {
+    ((a[k1 * R2 + n2] = rot<T, R1 * R2, n2 * k1, M>(u[k1], twM)), ...);
+}
+template <typename T, int R1, int R2, int M, int n2>
+__device__ __forceinline__ void ct_column(const C2<T>* v, C2<T>* a, const C2<T>* __restrict__ twM) {
+    C2<T> u[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) u[n1] = v[R2 * n1 + n2];
+    dft_plan<T, R1, M>(u, twM);
+    ct_twiddle<T, R1, R2, M, n2>(u, a, twM, std::make_integer_sequence<int, R1>{});
+}
+template <typename T, int R1, int R2, int M, int... n2>
+__device__ __forceinline__ void ct_columns(const C2<T>* v, C2<T>* a, const C2<T>* __restrict__ twM,
+                                           std::integer_sequence<int, n2...>) {
+    (ct_column<T, R1, R2, M, n2>(v, a, twM), ...);
+}
+template <typename T, int R1, int R2, int M>
+__device__ __forceinline__ void dft_ct(C2<T>* v, const C2<T>* __restrict__ twM) {
+    C2<T> a[R1 * R2];
+    ct_columns<T, R1, R2, M>(v, a, twM, std::make_integer_sequence<int, R2>{});
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+        C2<T> u[R2];
+#pragma unroll
+        for (int n2 = 0; n2 < R2; ++n2) u[n2] = a[k1 * R2 + n2];
+        dft_plan<T, R2, M>(u, twM);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = u[k2];
+    }
+}
+
+// Forward radix-R DFT of v[0..R-1] for any radix of a plan of length M.
+template <typename T, int R, int M>
+__device__ __forceinline__ void dft_plan(C2<T>* v, const C2<T>* __restrict__ twM) {
+    if constexpr (R == 16 || R == 8 || R == 4 || R == 2) dft_r<T, R>(v);
+    else if constexpr (R == 3) Dft<T, 3>::run(v, nullptr, 0);
+    else if constexpr (R == 5 || R == 7 || R == 11 || R == 13) Dft<T, R>::run(v, twM, M);
+    else if constexpr (R == 9) dft_ct<T, 3, 3, M>(v, twM);
+    else if constexpr (R == 10) dft_ct<T, 2, 5, M>(v, twM);
+    else if constexpr (R == 12) dft_ct<T, 4, 3, M>(v, twM);
+    else if constexpr (R == 14) dft_ct<T, 2, 7, M>(v, twM);
+    else if constexpr (R == 18) dft_ct<T, 2, 9, M>(v, twM);
+    else if constexpr (R == 20) dft_ct<T, 4, 5, M>(v, twM);
+    else static_assert(R == 16, "radix without a register DFT");
+}
+
 // Radix and Ns (product of the previous radices) of stage S.
 template <int M, int S>
 struct StageOf {
-    static constexpr int r = (S < Cfg<M>::A16) ? 16 : Cfg<M>::R0;
-    static constexpr int Ns = (S == 0) ? 1 : (S == 1 ? 16 : 256);
+    __host__ __device__ static constexpr int ns() {
+        int p = 1;
+        for (int i = 0; i < S; ++i) p *= Plan<M>::radix(i);
+        return p;
+    }
+    static constexpr int r = Plan<M>::radix(S);
+    static constexpr int Ns = ns();
 };
 
 // Stockham butterfly bookkeeping for slot `slot`, butterfly b of stage S.
@@ -120,13 +238,14 @@ template <int M, int S>
 struct Bfly {
     static constexpr int r = StageOf<M, S>::r;
     static constexpr int Ns = StageOf<M, S>::Ns;
-    static constexpr int B = kR / r;
+    static constexpr int B = Plan<M>::V / r;
     static constexpr int nb = M / r;
+    static_assert(B * r == Plan<M>::V, "every radix divides the values per thread");
     __device__ static __forceinline__ int j(int slot, int b) { return slot * B + b; }
     __device__ static __forceinline__ int in_idx(int slot, int b, int k) { return j(slot, b) + k * nb; }
     __device__ static __forceinline__ int out_idx(int slot, int b, int k) {
         const int jj = j(slot, b);
-        const int p = jj & (Ns - 1);
+        const int p = jj % Ns;
         return (jj - p) * r + p + k * Ns;
     }
 };
@@ -139,12 +258,12 @@ __device__ __forceinline__ void stage_compute(C2<T>* v, int slot, const C2<T>* _
 #pragma unroll
     for (int b = 0; b < BF::B; ++b) {
         if constexpr (BF::Ns > 1) {
-            const int p = BF::j(slot, b) & (BF::Ns - 1);
+            const int p = BF::j(slot, b) % BF::Ns;
             constexpr int tstep = M / (BF::Ns * r);
 #pragma unroll
             for (int k = 1; k < r; ++k) v[b * r + k] = cmul<T>(v[b * r + k], ldtw<T>(twM + p * k * tstep));
         }
-        dft_r<T, r>(v + b * r);
+        dft_plan<T, r, M>(v + b * r, twM);
     }
 }
 
@@ -234,8 +353,9 @@ __device__ __forceinline__ void transform_lines_v(const V& X, T* buf, T* red, in
     constexpr int M = CF::M;
     constexpr int W = CF::W, N = CF::N, P = CF::P;
     constexpr bool FWD = (KIND == kR2C || KIND == kDCT2 || KIND == kDST2);
+    constexpr int VPT = CF::V;
     C2<T>* Z = reinterpret_cast<C2<T>*>(buf);
-    C2<T> v[kR];
+    C2<T> v[VPT];
 
     // DCT1: partial sums of the odd entries x[1], x[3], ..., x[N-1] -- the
     // entries x[2n + 1] the pre step reads for this thread's inputs n, so the
@@ -254,7 +374,7 @@ __device__ __forceinline__ void transform_lines_v(const V& X, T* buf, T* red, in
     {
         using BF = Bfly<M, 0>;
 #pragma unroll
-        for (int k = 0; k < kR; ++k) v[k] = pre_value<T, KIND, M>(X, BF::in_idx(slot, 0, k), tb);
+        for (int k = 0; k < VPT; ++k) v[k] = pre_value<T, KIND, M>(X, BF::in_idx(slot, 0, k), tb);
         if constexpr (KIND == kDCT1) red[slot * W + c] = acc;
         CF::sync();
         stage_compute<T, M, 0>(v, slot, tb.twM);
@@ -275,8 +395,10 @@ __device__ __forceinline__ void transform_lines_v(const V& X, T* buf, T* red, in
         CF::sync();                                                                      \
         stage_compute<T, M, S>(v, slot, tb.twM);                                              \
     }
+    static_assert(CF::NST <= 4, "at most four stages");
     CHZ_STAGE(1)
     CHZ_STAGE(2)
+    CHZ_STAGE(3)
 #undef CHZ_STAGE
 
     // ---- post step ----
@@ -298,7 +420,7 @@ __device__ __forceinline__ void transform_lines_v(const V& X, T* buf, T* red, in
             for (int k = 0; k < LB::r; ++k) {
                 const int m = LB::out_idx(slot, b, k);
                 const C2<T> zk = v[b * LB::r + k];
-                const C2<T> zm = Z[CF::zi((M - m) & (M - 1), c)];
+                const C2<T> zm = Z[CF::zi(m == 0 ? 0 : M - m, c)];
                 const C2<T> wk = ldtw<T>(tb.twN + m);
                 const C2<T> e = cadd<T>(zk, cconj<T>(zm));
                 const C2<T> o = cmul<T>(wk, csub<T>(zk, cconj<T>(zm)));
@@ -333,7 +455,7 @@ __device__ __forceinline__ void transform_lines_v(const V& X, T* buf, T* red, in
             }
     } else if constexpr (KIND == kDCT1 || KIND == kDST1) {
         // v[n] = Re conj(Z[n/2]) (n even), Im conj(Z[n/2]) (n odd); pairs (k, N-k)
-        T outs[2 * kR];
+        T outs[2 * VPT];
         T S = T(0);
         if constexpr (KIND == kDCT1) {
             if (slot == 0) {
@@ -487,8 +609,13 @@ struct SmemLayout {
     static constexpr size_t total = ez + (FUSED ? sizeof(double) * (2 * M + 2) : 0);
 };
 
+// Four CTAs per SM (128 registers a thread); three for plans of more than 16
+// values a thread.
+template <int M>
+constexpr int fast_min_ctas() { return Plan<M>::V > kR ? 3 : 4; }
+
 template <typename T, typename TI, typename TO, int M, bool CONTIG, int KIND, int KIND2>
-__global__ void __launch_bounds__(kNT, 4)
+__global__ void __launch_bounds__(kNT, fast_min_ctas<M>())
 fast_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tg, int ntx, int ntiles) {
     using CF = Cfg<M>;
     using SL = SmemLayout<T, M, (KIND2 >= 0)>;

@@ -20,6 +20,7 @@
 #include <mutex>
 #include <string>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 #include "chz_internal.h"
@@ -267,8 +268,21 @@ static int launch_typed(const void* in, void* out, const PassArgs& a, const Devi
     return (int)cudaGetLastError();
 }
 
-// Power-of-two half lengths 16..512 use the register-resident kernels (FP64).
-bool fast_path_supported(int M) { return M >= 16 && M <= 512 && (M & (M - 1)) == 0; }
+// Power-of-two half lengths 16..512 use the register-resident kernels (FP64
+// and FP32); the mixed lengths with a register radix plan use them in FP64.
+static bool fast_mixed_length(int M) {
+    switch (M) {
+        case 12: case 20: case 24: case 28: case 40: case 48: case 56: case 72: case 80: case 96: case 160:
+        case 192:
+            return true;
+        default:
+            return false;
+    }
+}
+bool fast_path_supported(int M, bool is_double) {
+    if (M >= 16 && M <= 512 && (M & (M - 1)) == 0) return true;
+    return is_double && fast_mixed_length(M);
+}
 
 namespace fast {
 template <typename T, typename TI, typename TO, int M>
@@ -303,8 +317,27 @@ static int launch_fast_t(bool contig, const void* in, void* out, const PassArgs&
         CHZ_M(128);
         CHZ_M(256);
         CHZ_M(512);
-        default: return (int)cudaErrorInvalidValue;
+        default: break;
     }
+    if constexpr (std::is_same<T, double>::value && std::is_same<TI, double>::value &&
+                  std::is_same<TO, double>::value) {
+        switch (tb.M) {
+            CHZ_M(12);
+            CHZ_M(20);
+            CHZ_M(24);
+            CHZ_M(28);
+            CHZ_M(40);
+            CHZ_M(48);
+            CHZ_M(56);
+            CHZ_M(72);
+            CHZ_M(80);
+            CHZ_M(96);
+            CHZ_M(160);
+            CHZ_M(192);
+            default: break;
+        }
+    }
+    return (int)cudaErrorInvalidValue;
 #undef CHZ_M
 }
 
@@ -326,8 +359,16 @@ static int try_tma(const void* in, void* out, const PassArgs& a, const DeviceLin
         case 64: return tma::launch_tma_kind<T, 64>(a.kind, a.kind2, in, out, a, t, nv, stream, label);
         case 128: return tma::launch_tma_kind<T, 128>(a.kind, a.kind2, in, out, a, t, nv, stream, label);
         case 256: return tma::launch_tma_kind<T, 256>(a.kind, a.kind2, in, out, a, t, nv, stream, label);
-        default: return -1;
+        default: break;
     }
+    if constexpr (std::is_same<T, double>::value) {
+        switch (tb.M) {
+            case 96: return tma::launch_tma_kind<T, 96>(a.kind, a.kind2, in, out, a, t, nv, stream, label);
+            case 160: return tma::launch_tma_kind<T, 160>(a.kind, a.kind2, in, out, a, t, nv, stream, label);
+            default: break;
+        }
+    }
+    return -1;
 }
 
 namespace xtma {
@@ -361,7 +402,7 @@ int launch_line_pass(int is_double, int in_type, int out_type, bool contig, cons
                                  : try_tma<float>(in, out, a, tb, nv, stream, label);
         if (rc != -1) return rc;
     }
-    if (fast_path_supported(tb.M) && family != 1) {
+    if (fast_path_supported(tb.M, is_double != 0) && family != 1) {
         if (is_double) {
             if (in_type == kIoF64 && out_type == kIoF64)
                 return launch_fast_t<double, double, double>(contig, in, out, a, tb, nv, stream, label);

@@ -55,6 +55,11 @@ struct UsesDctTables {
 
 constexpr int kStages = 3;
 
+// Stage buffers of the strided pass: three for the power-of-two lengths; two
+// for the mixed ones, so that two CTAs fit an SM at N = 320.
+template <int M>
+constexpr int tma_stages() { return (M & (M - 1)) == 0 ? kStages : 2; }
+
 // Host-computed geometry of one pass.
 struct TmaGeom {
     int rows_buf;     // rows of one stage buffer
@@ -326,9 +331,10 @@ __device__ __forceinline__ void r2c_div_c2r_regs(T* buf, int c, int slot, bool p
 template <typename T, int M, bool FUSED, bool DCTTAB = true>
 struct TmaSmem {
     using CF = TCfg<T, M>;
+    static constexpr int NS = tma_stages<M>();
     __host__ __device__ static constexpr size_t al(size_t b, size_t a) { return (b + a - 1) / a * a; }
     __host__ __device__ static size_t stage_bytes(int rows_buf) { return (size_t)rows_buf * CF::W * sizeof(T); }
-    __host__ __device__ static size_t twM(int rows_buf) { return al(kStages * stage_bytes(rows_buf), 128); }
+    __host__ __device__ static size_t twM(int rows_buf) { return al(NS * stage_bytes(rows_buf), 128); }
     __host__ __device__ static size_t twN(int rows_buf) { return twM(rows_buf) + sizeof(C2<T>) * M; }
     __host__ __device__ static size_t tw4N(int rows_buf) { return twN(rows_buf) + sizeof(C2<T>) * (M + 1); }
     __host__ __device__ static size_t inv4sin(int rows_buf) {
@@ -341,18 +347,25 @@ struct TmaSmem {
         return al(ez(rows_buf) + (FUSED ? sizeof(double) * (2 * M + 2) : 0), 16);
     }
     __host__ __device__ static size_t bars(int rows_buf) { return al(red(rows_buf) + sizeof(T) * CF::RED, 16); }
-    __host__ __device__ static size_t abort(int rows_buf) { return bars(rows_buf) + 2 * kStages * sizeof(uint64_t); }
+    __host__ __device__ static size_t abort(int rows_buf) { return bars(rows_buf) + 2 * NS * sizeof(uint64_t); }
     __host__ __device__ static size_t total(int rows_buf) { return abort(rows_buf) + 16; }
 };
 
+// One CTA per SM asked of the compiler for the power-of-two lengths (the
+// pipeline's shared memory allows no more at N = 512), two for the mixed ones
+// (smaller tiles, fewer compute warps a CTA).
+template <int M>
+constexpr int tma_min_ctas() { return (M & (M - 1)) == 0 ? 1 : 2; }
+
 template <typename T, int M, int KIND, int KIND2>
-__global__ void __launch_bounds__(TCfg<T, M>::NT + 32, 1)
+__global__ void __launch_bounds__(TCfg<T, M>::NT + 32, tma_min_ctas<M>())
 tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUtensorMap stmap, PassArgs a,
          LineTables<T> tg, TmaGeom g, int ntx, int ntiles, int* flags, long long wait_limit) {
     using CF = TCfg<T, M>;
     constexpr bool DCTTAB = UsesDctTables<KIND, KIND2>::value;
     using SL = TmaSmem<T, M, (KIND2 >= 0), DCTTAB>;
     constexpr int W = CF::W, PR = CF::PR, NT = CF::NT, N = CF::N;
+    constexpr int NS = SL::NS;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int t = threadIdx.x;
     if ((int)blockIdx.x >= ntiles) return;
@@ -363,7 +376,7 @@ tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUte
     const int rb = g.rows_buf;
     const size_t sbytes = SL::stage_bytes(rb);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + SL::bars(rb));
-    uint64_t* ready = full + kStages;
+    uint64_t* ready = full + NS;
     volatile int* abort = reinterpret_cast<volatile int*>(smem_raw + SL::abort(rb));
     T* red = reinterpret_cast<T*>(smem_raw + SL::red(rb));
 
@@ -394,7 +407,7 @@ tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUte
     }
     if (t == 0) {
         *abort = 0;
-        for (int s = 0; s < kStages; ++s) {
+        for (int s = 0; s < NS; ++s) {
             mbar_init(full + s, 1);
             mbar_init(ready + s, NT);
         }
@@ -410,7 +423,7 @@ tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUte
         asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&ldmap)) : "memory");
         asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&stmap)) : "memory");
         auto issue_load = [&](int i) {
-            const int s = i % kStages;
+            const int s = i % NS;
             const int tile = (int)blockIdx.x + i * (int)gridDim.x;
             const int cx = (tile % ntx) * W;
             const int v = a.v0 + tile / ntx - g.v_off;   // map coordinate
@@ -423,11 +436,11 @@ tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUte
                 else tma_load(d, &ldmap, cx, v, l, full + s);
             }
         };
-        const int pre = nloc < kStages ? nloc : kStages;
+        const int pre = nloc < NS ? nloc : NS;
         for (int i = 0; i < pre; ++i) issue_load(i);
         for (int i = 0; i < nloc; ++i) {
-            const int s = i % kStages;
-            if (!mbar_wait(ready + s, (uint32_t)((i / kStages) & 1), abort, wait_limit))
+            const int s = i % NS;
+            if (!mbar_wait(ready + s, (uint32_t)((i / NS) & 1), abort, wait_limit))
                 atomicOr(flags, kFlagProducer);
             const int tile = (int)blockIdx.x + i * (int)gridDim.x;
             const int cx = (tile % ntx) * W;
@@ -440,14 +453,14 @@ tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUte
                 else tma_store(&stmap, cx, v, l, sp);
             }
             asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
-            if (i + kStages < nloc) {
+            if (i + NS < nloc) {
                 // the buffer is refilled once the store has read it
                 asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
-                issue_load(i + kStages);
+                issue_load(i + NS);
             }
         }
         asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
-        drain_loads(full, nloc, kStages, wait_limit, flags);
+        drain_loads(full, nloc, NS, wait_limit, flags);
         return;
     }
 
@@ -456,8 +469,8 @@ tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUte
     const int c = t % W;
     const int slot = REGSPEC ? paired_slot<CF::P>(t) : t / W;
     for (int i = 0; i < nloc; ++i) {
-        const int s = i % kStages;
-        if (!mbar_wait(full + s, (uint32_t)((i / kStages) & 1), abort, wait_limit)) {
+        const int s = i % NS;
+        if (!mbar_wait(full + s, (uint32_t)((i / NS) & 1), abort, wait_limit)) {
             if (t == 0) atomicOr(flags, kFlagConsumer);
         }
         T* buf = reinterpret_cast<T*>(smem_raw + (size_t)s * sbytes);

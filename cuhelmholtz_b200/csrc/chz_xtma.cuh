@@ -60,6 +60,7 @@ struct SwzView {
 template <int M_>
 struct XCfg {
     static constexpr int M = M_;
+    static constexpr int V = fast::kR;
     static constexpr int P = M / fast::kR;
     static constexpr int W = 16;
     static constexpr int NT = P * W;
