@@ -719,10 +719,10 @@ def measure_batch(args, count, steps):
     targets, tuned_ms = plan.tiles()
     schedules = plan.radix_schedules()
     mode, mode_ms = plan.launch_mode()
-    periodic = any(0 in (p["xbc"], p["ybc"], p["zbc"]) for p in probs)
-    # kernels in one graph replay: the persistent kernel, or five passes and
-    # the periodic planes
-    kernels_per_solve = 1 if mode == 0 else 5 + (1 if periodic else 0)
+    # kernels in one graph replay: the persistent kernel, or per pass the
+    # register-resident group launches and the leftover launch, and the
+    # periodic planes
+    kernels_per_solve = plan.kernels()
     # the same batch with the untuned tile size (4096 values per tile)
     prev = chz.BatchPlan.set_autotune(False)
     try:
@@ -760,8 +760,10 @@ def measure_batch(args, count, steps):
             "model": "80 B per point (five passes of 16 B)",
             "loop_of_single_solves": {"value": loop_value, "ms_per_step": ms_loop / steps},
             "launch": ("one persistent kernel over a work queue of (pass, problem, tile) items"
-                       if mode == 0 else "one launch per pass over all problems, then the periodic planes")
+                       if mode == 0 else "per pass, one register-resident launch per group of problems with the "
+                       "same line length and kinds and one generic launch over the rest, then the periodic planes")
                       + ", replayed from a CUDA graph",
+            "kernels_per_solve": kernels_per_solve,
             "launch_form_ms": {"persistent": mode_ms[0], "per_pass": mode_ms[1],
                                "chosen": "persistent" if mode == 0 else "per_pass"},
             "autotune": {"tile_values_per_pass": targets, "tuned_ms_per_pass": tuned_ms,

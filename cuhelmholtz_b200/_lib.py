@@ -66,6 +66,7 @@ SIGNATURES = {
     "chz_batch_set_radix_schedule": (c_int, [c_int]),
     "chz_batch_plan_launch": (c_int, [c_void_p, c_void_p, c_void_p]),
     "chz_batch_set_launch_mode": (c_int, [c_int]),
+    "chz_batch_plan_kernels": (c_int, [c_void_p]),
     "chz_helmholtz_solve_noalloc": (c_int, [c_double, c_double, c_int, c_int, _dp, _dp,
                                             c_double, c_double, c_int, c_int, _dp, _dp,
                                             c_double, c_double, c_int, c_int, _dp, _dp,

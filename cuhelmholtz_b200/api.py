@@ -253,9 +253,19 @@ class BatchPlan:
         _check(_lib.lib().chz_batch_plan_radix(self._handle, v))
         return list(v)
 
+    def kernels(self) -> int:
+        """Kernel launches one solve of this plan replays (1 in the persistent
+        form; per pass its register-resident groups and leftover launch, plus
+        the periodic planes, in the per-pass form)."""
+        n = int(_lib.lib().chz_batch_plan_kernels(self._handle))
+        if n < 0:
+            _check(n)
+        return n
+
     def launch_mode(self):
-        """The plan's launch form (0: one persistent launch; 1: a launch per
-        pass) and the measured ms of one batched solve in each ([0, 0]: not
+        """The plan's launch form (0: one persistent launch; 1: launches per
+        pass, register-resident groups and the generic kernel for the rest)
+        and the measured ms of one batched solve in each ([0, 0]: not
         timed)."""
         import ctypes
         m = ctypes.c_int()

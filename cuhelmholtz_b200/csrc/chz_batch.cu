@@ -43,10 +43,7 @@ namespace {
 
 constexpr int kPasses = 5;
 
-struct ProbPtrs {
-    double* f;
-    const double* face[6];  // bcl, bcr, bcb, bct, bcf, bce
-};
+using ProbPtrs = BatchPtrs;
 
 struct BatchItem {
     PassArgs a;
@@ -72,15 +69,16 @@ __device__ __forceinline__ int find_problem(const int* start, int count, int b) 
     return lo;
 }
 
+// items[s] is the pass of problem prob[s] (prob == nullptr: of problem s).
 template <bool CONTIG>
 __global__ void __launch_bounds__(kThreads, 2)
 batch_pass(const BatchItem* __restrict__ items, const int* __restrict__ start, int count,
-           const ProbPtrs* __restrict__ ptrs, double* ws) {
+           const ProbPtrs* __restrict__ ptrs, double* ws, const int* __restrict__ prob) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int s = find_problem(start, count, blockIdx.x);
     const BatchItem& it = items[s];
     PassArgs a = it.a;
-    const ProbPtrs& p = ptrs[s];
+    const ProbPtrs& p = ptrs[prob ? prob[s] : s];
     if (a.has_bc) {
         a.bc.f = p.f;
         a.bc.bcl = p.face[0];
@@ -264,6 +262,17 @@ __global__ void __launch_bounds__(kThreads, 2) batch_persistent(PersistArgs A) {
 
 using namespace chz;
 
+// The problems of one pass that a register-resident kernel takes, grouped
+// by (length, kinds): one launch each.
+struct FastGroup {
+    int kind = 0, kind2 = -1;
+    chz::LineTables<double> tb{};
+    chz::BatchMember* members_d = nullptr;
+    int* start_d = nullptr;
+    int count = 0;
+    int ntiles = 0;
+};
+
 struct chz_batch_plan {
     int count = 0;
     int device = 0;
@@ -290,8 +299,17 @@ struct chz_batch_plan {
     int grid = 0;                        // CTAs of the persistent launch
     size_t smem_all = 0;                 // its dynamic shared memory
     bool periodic = false;               // some problem has a periodic axis
-    int mode = 0;                        // 0: one persistent launch; 1: a launch per pass
+    int mode = 0;                        // 0: one persistent launch; 1: launches per pass
     float mode_ms[2] = {};               // measured solve time of each form (0: not timed)
+    // launches per pass: the register-resident groups, then one launch of the
+    // generic kernel over the problems no group takes (the leftovers)
+    std::vector<FastGroup> groups[kPasses];
+    BatchItem* left_items_d[kPasses] = {};
+    int* left_start_d[kPasses] = {};
+    int* left_prob_d[kPasses] = {};
+    int left_count[kPasses] = {};
+    int left_tiles[kPasses] = {};
+    size_t left_smem[kPasses] = {};
 };
 
 namespace {
@@ -303,6 +321,13 @@ void free_plan(chz_batch_plan* p) {
     for (int q = 0; q < kPasses; ++q) {
         if (p->items_d[q]) cudaFree(p->items_d[q]);
         if (p->start_d[q]) cudaFree(p->start_d[q]);
+        for (FastGroup& g : p->groups[q]) {
+            if (g.members_d) cudaFree(g.members_d);
+            if (g.start_d) cudaFree(g.start_d);
+        }
+        if (p->left_items_d[q]) cudaFree(p->left_items_d[q]);
+        if (p->left_start_d[q]) cudaFree(p->left_start_d[q]);
+        if (p->left_prob_d[q]) cudaFree(p->left_prob_d[q]);
     }
     if (p->fix_d) cudaFree(p->fix_d);
     if (p->ptrs_d) cudaFree(p->ptrs_d);
@@ -392,15 +417,102 @@ void apply_variant(std::vector<BatchItem>& items, int variant) {
     }
 }
 
+cudaError_t raise_smem(bool contig, size_t bytes);
+
+// Pass q of every problem on the generic kernel (one launch).
 cudaError_t launch_pass(chz_batch_plan* p, int q, cudaStream_t s) {
     if (p->tiles[q] == 0) return cudaSuccess;
     if (p->contig[q])
         batch_pass<true><<<p->tiles[q], kThreads, p->smem[q], s>>>(p->items_d[q], p->start_d[q], p->count,
-                                                                   p->ptrs_d, p->ws);
+                                                                   p->ptrs_d, p->ws, nullptr);
     else
         batch_pass<false><<<p->tiles[q], kThreads, p->smem[q], s>>>(p->items_d[q], p->start_d[q], p->count,
-                                                                    p->ptrs_d, p->ws);
+                                                                    p->ptrs_d, p->ws, nullptr);
     return cudaGetLastError();
+}
+
+// Pass q as the per-pass form runs it: one register-resident launch per
+// group, then the generic kernel over the leftovers.
+cudaError_t launch_pass_grouped(chz_batch_plan* p, int q, cudaStream_t s) {
+    for (const FastGroup& g : p->groups[q]) {
+        FastBatchArgs A{g.members_d, g.start_d, g.count, g.ntiles, p->ptrs_d, p->ws};
+        const int rc = launch_fast_batch(p->contig[q], g.kind, g.kind2, A, g.tb, s);
+        if (rc != 0) return (cudaError_t)rc;
+    }
+    if (p->left_count[q] == 0 || p->left_tiles[q] == 0) return cudaSuccess;
+    if (p->contig[q])
+        batch_pass<true><<<p->left_tiles[q], kThreads, p->left_smem[q], s>>>(
+            p->left_items_d[q], p->left_start_d[q], p->left_count[q], p->ptrs_d, p->ws, p->left_prob_d[q]);
+    else
+        batch_pass<false><<<p->left_tiles[q], kThreads, p->left_smem[q], s>>>(
+            p->left_items_d[q], p->left_start_d[q], p->left_count[q], p->ptrs_d, p->ws, p->left_prob_d[q]);
+    return cudaGetLastError();
+}
+
+// Splits pass q into register-resident groups (problems whose line length has
+// a register plan, by (length, kinds)) and the leftovers, and uploads both.
+cudaError_t build_groups(chz_batch_plan* p, int q, const std::vector<PassTemplate>& tp,
+                         const std::vector<BatchItem>& items) {
+    std::map<std::tuple<int, int, int>, std::vector<int>> by_key;
+    std::vector<int> left;
+    for (int i = 0; i < p->count; ++i) {
+        const int n = tp[i].n;
+        const int M = n / 2;
+        const bool fast = (n % 2 == 0) && fast_path_supported(M, true) && fast_lines_per_tile(M) > 0;
+        if (fast) by_key[std::make_tuple(M, items[i].a.kind, items[i].a.kind2)].push_back(i);
+        else left.push_back(i);
+    }
+    cudaError_t e = cudaSuccess;
+    for (const auto& kv : by_key) {
+        const int M = std::get<0>(kv.first);
+        const int W = fast_lines_per_tile(M);
+        FastGroup g;
+        g.kind = std::get<1>(kv.first);
+        g.kind2 = std::get<2>(kv.first);
+        g.tb = items[kv.second[0]].tb;
+        std::vector<BatchMember> mem;
+        std::vector<int> start(1, 0);
+        for (int i : kv.second) {
+            BatchMember m{};
+            m.a = items[i].a;
+            m.prob = i;
+            m.ntx = (m.a.nu + W - 1) / W;
+            m.in_user = items[i].in_user;
+            m.out_user = items[i].out_user;
+            m.ws_off = items[i].ws_off;
+            mem.push_back(m);
+            start.push_back(start.back() + m.ntx * tp[i].nv);
+        }
+        g.count = (int)mem.size();
+        g.ntiles = start.back();
+        if (e == cudaSuccess) e = cudaMalloc(&g.members_d, sizeof(BatchMember) * mem.size());
+        if (e == cudaSuccess) e = cudaMalloc(&g.start_d, sizeof(int) * start.size());
+        if (e == cudaSuccess)
+            e = cudaMemcpy(g.members_d, mem.data(), sizeof(BatchMember) * mem.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(g.start_d, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice);
+        p->groups[q].push_back(g);   // freed with the plan even when an upload failed
+    }
+    p->left_count[q] = (int)left.size();
+    if (left.empty() || e != cudaSuccess) return e;
+    std::vector<BatchItem> li;
+    std::vector<int> ls(1, 0);
+    size_t smem = 0;
+    for (int i : left) {
+        li.push_back(items[i]);
+        ls.push_back(ls.back() + items[i].ntx * tp[i].nv);
+        const LineGeom geo = line_geometry_target(tp[i].n, 1, p->contig[q], p->target[q], kBatchMaxSmem);
+        smem = std::max(smem, geo.smem_bytes);
+    }
+    p->left_tiles[q] = ls.back();
+    p->left_smem[q] = smem;
+    e = cudaMalloc(&p->left_items_d[q], sizeof(BatchItem) * li.size());
+    if (e == cudaSuccess) e = cudaMalloc(&p->left_start_d[q], sizeof(int) * ls.size());
+    if (e == cudaSuccess) e = cudaMalloc(&p->left_prob_d[q], sizeof(int) * left.size());
+    if (e == cudaSuccess) e = cudaMemcpy(p->left_items_d[q], li.data(), sizeof(BatchItem) * li.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(p->left_start_d[q], ls.data(), sizeof(int) * ls.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(p->left_prob_d[q], left.data(), sizeof(int) * left.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = raise_smem(p->contig[q], smem);
+    return e;
 }
 
 // The dynamic shared-memory limit is an attribute of the kernel, shared by
@@ -534,7 +646,7 @@ cudaError_t prepare_persistent(chz_batch_plan* p) {
 int enqueue(chz_batch_plan* p, cudaStream_t s) {
     if (p->mode == 1) {
         for (int q = 0; q < kPasses; ++q) {
-            const cudaError_t e = launch_pass(p, q, s);
+            const cudaError_t e = launch_pass_grouped(p, q, s);
             if (e != cudaSuccess) return cuda_fail((int)e, "batched pass");
         }
         if (p->periodic) {
@@ -771,6 +883,7 @@ int chz_batch_plan_create(int count, const int* dims, const int* bcs, const doub
         materialise(tmpl[q], p->contig[q], p->target[q], items[q], start[q], &p->tiles[q], &p->smem[q]);
         apply_variant(items[q], p->plan_variant[q]);
         e = upload_pass(p, q, items[q], start[q]);
+        if (e == cudaSuccess) e = build_groups(p, q, tmpl[q], items[q]);
     }
     if (e == cudaSuccess) e = cudaMalloc(&p->counters, sizeof(int) * ((size_t)count * kPasses + 1));
     if (e == cudaSuccess) {
@@ -888,6 +1001,15 @@ int chz_batch_solve(chz_batch_plan* p, double* const* f, const double* const* fa
     trace_end(s);
     if (e != cudaSuccess) return cuda_fail((int)e, "graph launch");
     return CHZ_SUCCESS;
+}
+
+int chz_batch_plan_kernels(const chz_batch_plan* plan) {
+    if (!plan) return fail(CHZ_ERROR_INVALID_VALUE, "NULL plan");
+    if (plan->mode == 0) return 1;
+    int n = plan->periodic ? 1 : 0;
+    for (int q = 0; q < kPasses; ++q)
+        n += (int)plan->groups[q].size() + ((plan->left_count[q] > 0 && plan->left_tiles[q] > 0) ? 1 : 0);
+    return n;
 }
 
 int chz_batch_plan_destroy(chz_batch_plan* plan) {

@@ -614,6 +614,133 @@ struct SmemLayout {
 template <int M>
 constexpr int fast_min_ctas() { return Plan<M>::V > kR ? 3 : 4; }
 
+// One tile of a pass: load (cp.async), boundary terms, the line transforms
+// (with the division of a fused pass) and the store.  `a` may live in the
+// kernel's parameters or in shared memory (the batched kernel).
+template <typename T, typename TI, typename TO, int M, bool CONTIG, int KIND, int KIND2>
+__device__ __forceinline__ void fast_tile(const TI* in, TO* out, const PassArgs& a, const LineTables<T>& tb,
+                                          const double* ez_s, T* buf, T* red, int tile, int ntx, int t, int c,
+                                          int slot) {
+    using CF = Cfg<M>;
+    constexpr int W = CF::W, PR = CF::PR, P = CF::P, N = CF::N;
+    const int tx = tile % ntx;
+    const int v = a.v0 + tile / ntx;
+    const int ub = a.u0 + tx * W;
+    const int nl = min(W, a.u0 + a.nu - ub);
+    load_tile<T, TI, M, CONTIG, KIND>(buf, in, a, ub, nl, v, t, c, slot);
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+
+    if (CONTIG && a.has_bc) {
+        // boundary terms: every entry of a y/z boundary row; elsewhere the
+        // entries at xs and xe (one thread applies all terms of an entry)
+        const BcArgs& b = a.bc;
+        const bool zrow = (v == b.zs || v == b.ze);
+        // rows on a y or z boundary: every entry
+        for (int cc = 0; cc < nl; ++cc) {
+            const int j = ub + cc;
+            if (zrow || j == b.ys || j == b.ye) {
+                for (int l = a.ld_lo + t; l <= a.ld_hi; l += kNT)
+                    buf[l * PR + cc] = (T)bc_terms((double)buf[l * PR + cc], b, l, j, v);
+            }
+        }
+        // other rows: the entries at xs and xe, one (row, side) per thread
+        for (int q = t; q < 2 * nl; q += kNT) {
+            const int cc = q >> 1;
+            const int j = ub + cc;
+            if (zrow || j == b.ys || j == b.ye) continue;
+            if ((q & 1) && b.xe == b.xs) continue;
+            const int l = (q & 1) ? b.xe : b.xs;
+            buf[l * PR + cc] = (T)bc_terms((double)buf[l * PR + cc], b, l, j, v);
+        }
+        __syncthreads();
+    }
+
+    if constexpr (KIND2 >= 0) {
+        OutSink<T, PR, true> s1;
+        s1.Rv = buf;
+        s1.c = c;
+        const int i = min(ub + c, a.u0 + a.nu - 1);
+        s1.exy = __ldg(a.dv.ex + i) + __ldg(a.dv.ey + v);
+        s1.lam = a.dv.lambda;
+        s1.ez = ez_s;
+        s1.dlo = a.dv.lo;
+        s1.dhi = a.dv.hi;
+        s1.zmax = (a.dv.perturb && i <= a.dv.xz_hi && v <= a.dv.yz_hi) ? a.dv.zz_hi : -1;
+        transform_lines<T, CF, KIND>(buf, red, c, slot, tb, s1);
+        OutSink<T, PR, false> s2;
+        s2.Rv = buf;
+        s2.c = c;
+        transform_lines<T, CF, KIND2>(buf, red, c, slot, tb, s2);
+    } else {
+        OutSink<T, PR, false> s;
+        s.Rv = buf;
+        s.c = c;
+        transform_lines<T, CF, KIND>(buf, red, c, slot, tb, s);
+    }
+
+    // ---- store the output window ----
+    {
+        const int lo = a.st_lo, hi = a.st_hi;
+        const long long vb = (long long)v * a.out_sv;
+        const double sc = a.use_scale ? a.scale : 1.0;
+        if constexpr (CONTIG) {
+            // accumulated output (the refinement's update u += c): all of
+            // a thread's u values are loaded before any store, so the
+            // loads overlap instead of one latency per row
+            constexpr int NI = (N + 2 + kNT - 1) / kNT;
+            bool done = false;
+            if constexpr (W * NI <= 48) {
+                if (a.acc) {
+                    double av[W][NI];
+#pragma unroll
+                    for (int cc = 0; cc < W; ++cc) {
+                        const double* arow = a.acc + vb + (long long)(ub + cc) * a.out_su;
+#pragma unroll
+                        for (int it = 0; it < NI; ++it) {
+                            const int l = lo + t + it * kNT;
+                            av[cc][it] = (cc < nl && l <= hi) ? __ldg(arow + l) : 0.0;
+                        }
+                    }
+#pragma unroll
+                    for (int cc = 0; cc < W; ++cc) {
+                        TO* row = out + vb + (long long)(ub + cc) * a.out_su;
+#pragma unroll
+                        for (int it = 0; it < NI; ++it) {
+                            const int l = lo + t + it * kNT;
+                            if (cc < nl && l <= hi) row[l] = (TO)(av[cc][it] + (double)buf[l * PR + cc] * sc);
+                        }
+                    }
+                    done = true;
+                }
+            }
+#pragma unroll 1
+            for (int cc = 0; cc < (done ? 0 : nl); ++cc) {
+                const long long ro = vb + (long long)(ub + cc) * a.out_su;
+                TO* row = out + ro;
+                if (a.acc) {
+                    const double* arow = a.acc + ro;
+                    for (int l = lo + t; l <= hi; l += kNT) row[l] = (TO)(arow[l] + (double)buf[l * PR + cc] * sc);
+                } else {
+                    for (int l = lo + t; l <= hi; l += kNT) row[l] = (TO)((double)buf[l * PR + cc] * sc);
+                }
+            }
+        } else if (c < nl) {
+            const long long o = vb + (long long)(ub + c) * a.out_su + (long long)(lo + slot) * a.out_sl;
+            TO* p = out + o;
+            const double* q = a.acc ? a.acc + o : nullptr;
+            const long long step = (long long)P * a.out_sl;
+            for (int l = lo + slot; l <= hi; l += P) {
+                const double x = (double)buf[l * PR + c] * sc;
+                *p = (TO)(q ? *q + x : x);
+                p += step;
+                if (q) q += step;
+            }
+        }
+    }
+    __syncthreads();
+}
+
 template <typename T, typename TI, typename TO, int M, bool CONTIG, int KIND, int KIND2>
 __global__ void __launch_bounds__(kNT, fast_min_ctas<M>())
 fast_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tg, int ntx, int ntiles) {
@@ -658,124 +785,110 @@ fast_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tg, int ntx, int ntil
         for (int i = t; i < N + 2; i += kNT) ez_s[i] = a.dv.ez[i];
     }
 
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const int tx = tile % ntx;
-        const int v = a.v0 + tile / ntx;
-        const int ub = a.u0 + tx * W;
-        const int nl = min(W, a.u0 + a.nu - ub);
-        load_tile<T, TI, M, CONTIG, KIND>(buf, in, a, ub, nl, v, t, c, slot);
-        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-        __syncthreads();
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+        fast_tile<T, TI, TO, M, CONTIG, KIND, KIND2>(in, out, a, tb, ez_s, buf, red, tile, ntx, t, c, slot);
+}
 
-        if (CONTIG && a.has_bc) {
-            // boundary terms: every entry of a y/z boundary row; elsewhere the
-            // entries at xs and xe (one thread applies all terms of an entry)
-            const BcArgs& b = a.bc;
-            const bool zrow = (v == b.zs || v == b.ze);
-            // rows on a y or z boundary: every entry
-            for (int cc = 0; cc < nl; ++cc) {
-                const int j = ub + cc;
-                if (zrow || j == b.ys || j == b.ye) {
-                    for (int l = a.ld_lo + t; l <= a.ld_hi; l += kNT)
-                        buf[l * PR + cc] = (T)bc_terms((double)buf[l * PR + cc], b, l, j, v);
-                }
+// One group of a batched pass (FP64): the members share the length and the
+// kinds, so the line tables are staged once; each CTA takes a contiguous range
+// of the group's tiles and, when the member changes, copies that member's pass
+// descriptor into shared memory (its f and face pointers patched from the
+// call's pointer table) and stages its z eigenvalue terms (fused pass).
+template <int M, bool CONTIG, int KIND, int KIND2>
+__global__ void __launch_bounds__(kNT, fast_min_ctas<M>())
+fast_batch_pass(FastBatchArgs g, LineTables<double> tg) {
+    using T = double;
+    using CF = Cfg<M>;
+    using SL = SmemLayout<T, M, (KIND2 >= 0)>;
+    constexpr int W = CF::W, N = CF::N;
+    constexpr size_t kArgs = (SL::total + 15) & ~size_t(15);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ const double* s_in;
+    __shared__ double* s_out;
+    __shared__ int s_ntx, s_first;
+    T* buf = reinterpret_cast<T*>(smem_raw + SL::buf);
+    T* red = reinterpret_cast<T*>(smem_raw + SL::red);
+    PassArgs* as = reinterpret_cast<PassArgs*>(smem_raw + kArgs);
+
+    const int t = threadIdx.x;
+    const int c = t % W;
+    constexpr bool spread = CONTIG && W == 8;
+    const int slot = spread ? (t >> 5) + (kNT / 32) * ((t & 31) / W) : t / W;
+    const int per = (g.ntiles + (int)gridDim.x - 1) / (int)gridDim.x;
+    const int t0 = (int)blockIdx.x * per;
+    const int t1 = min(g.ntiles, t0 + per);
+    if (t0 >= t1) return;
+
+    LineTables<T> tb = tg;
+    {
+        C2<T>* sM = reinterpret_cast<C2<T>*>(smem_raw + SL::twM);
+        C2<T>* sN = reinterpret_cast<C2<T>*>(smem_raw + SL::twN);
+        C2<T>* s4 = reinterpret_cast<C2<T>*>(smem_raw + SL::tw4N);
+        T* sI = reinterpret_cast<T*>(smem_raw + SL::inv4sin);
+        for (int i = t; i < M; i += kNT) sM[i] = tg.twM[i];
+        for (int i = t; i <= M; i += kNT) {
+            sN[i] = tg.twN[i];
+            s4[i] = tg.tw4N[i];
+            sI[i] = tg.inv4sin[i];
+        }
+        tb.twM = sM;
+        tb.twN = sN;
+        tb.tw4N = s4;
+        tb.inv4sin = sI;
+    }
+    double* ez_s = reinterpret_cast<double*>(smem_raw + SL::ez);
+
+    int cur = -1, cur_end = 0;
+    for (int tile = t0; tile < t1; ++tile) {
+        if (tile >= cur_end) {
+            // the member owning this tile (binary search over the prefix)
+            int lo = 0, hi = g.count - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (__ldg(g.start + mid) <= tile) lo = mid;
+                else hi = mid - 1;
             }
-            // other rows: the entries at xs and xe, one (row, side) per thread
-            for (int q = t; q < 2 * nl; q += kNT) {
-                const int cc = q >> 1;
-                const int j = ub + cc;
-                if (zrow || j == b.ys || j == b.ye) continue;
-                if ((q & 1) && b.xe == b.xs) continue;
-                const int l = (q & 1) ? b.xe : b.xs;
-                buf[l * PR + cc] = (T)bc_terms((double)buf[l * PR + cc], b, l, j, v);
+            cur = lo;
+            cur_end = __ldg(g.start + cur + 1);
+            __syncthreads();   // every thread is done with the previous member's descriptor
+            const BatchMember* mb = g.members + cur;
+            const long long* src = reinterpret_cast<const long long*>(&mb->a);
+            long long* dst = reinterpret_cast<long long*>(as);
+            static_assert(sizeof(PassArgs) % 8 == 0, "descriptor copied in 8-byte words");
+            for (int i = t; i < (int)(sizeof(PassArgs) / 8); i += kNT) dst[i] = __ldg(src + i);
+            __syncthreads();
+            if (t == 0) {
+                const BatchPtrs& pp = g.ptrs[mb->prob];
+                if (as->has_bc) {
+                    as->bc.f = pp.f;
+                    as->bc.bcl = pp.face[0];
+                    as->bc.bcr = pp.face[1];
+                    as->bc.bcb = pp.face[2];
+                    as->bc.bct = pp.face[3];
+                    as->bc.bcf = pp.face[4];
+                    as->bc.bce = pp.face[5];
+                }
+                s_in = mb->in_user ? pp.f : g.ws + mb->ws_off;
+                s_out = mb->out_user ? pp.f : g.ws + mb->ws_off;
+                s_ntx = mb->ntx;
+                s_first = __ldg(g.start + cur);
+            }
+            if constexpr (KIND2 >= 0) {
+                const double* ez = mb->a.dv.ez;
+                for (int i = t; i < N + 2; i += kNT) ez_s[i] = __ldg(ez + i);
             }
             __syncthreads();
         }
-
-        if constexpr (KIND2 >= 0) {
-            OutSink<T, PR, true> s1;
-            s1.Rv = buf;
-            s1.c = c;
-            const int i = min(ub + c, a.u0 + a.nu - 1);
-            s1.exy = __ldg(a.dv.ex + i) + __ldg(a.dv.ey + v);
-            s1.lam = a.dv.lambda;
-            s1.ez = ez_s;
-            s1.dlo = a.dv.lo;
-            s1.dhi = a.dv.hi;
-            s1.zmax = (a.dv.perturb && i <= a.dv.xz_hi && v <= a.dv.yz_hi) ? a.dv.zz_hi : -1;
-            transform_lines<T, CF, KIND>(buf, red, c, slot, tb, s1);
-            OutSink<T, PR, false> s2;
-            s2.Rv = buf;
-            s2.c = c;
-            transform_lines<T, CF, KIND2>(buf, red, c, slot, tb, s2);
-        } else {
-            OutSink<T, PR, false> s;
-            s.Rv = buf;
-            s.c = c;
-            transform_lines<T, CF, KIND>(buf, red, c, slot, tb, s);
-        }
-
-        // ---- store the output window ----
-        {
-            const int lo = a.st_lo, hi = a.st_hi;
-            const long long vb = (long long)v * a.out_sv;
-            const double sc = a.use_scale ? a.scale : 1.0;
-            if constexpr (CONTIG) {
-                // accumulated output (the refinement's update u += c): all of
-                // a thread's u values are loaded before any store, so the
-                // loads overlap instead of one latency per row
-                constexpr int NI = (N + 2 + kNT - 1) / kNT;
-                bool done = false;
-                if constexpr (W * NI <= 48) {
-                    if (a.acc) {
-                        double av[W][NI];
-#pragma unroll
-                        for (int cc = 0; cc < W; ++cc) {
-                            const double* arow = a.acc + vb + (long long)(ub + cc) * a.out_su;
-#pragma unroll
-                            for (int it = 0; it < NI; ++it) {
-                                const int l = lo + t + it * kNT;
-                                av[cc][it] = (cc < nl && l <= hi) ? __ldg(arow + l) : 0.0;
-                            }
-                        }
-#pragma unroll
-                        for (int cc = 0; cc < W; ++cc) {
-                            TO* row = out + vb + (long long)(ub + cc) * a.out_su;
-#pragma unroll
-                            for (int it = 0; it < NI; ++it) {
-                                const int l = lo + t + it * kNT;
-                                if (cc < nl && l <= hi) row[l] = (TO)(av[cc][it] + (double)buf[l * PR + cc] * sc);
-                            }
-                        }
-                        done = true;
-                    }
-                }
-#pragma unroll 1
-                for (int cc = 0; cc < (done ? 0 : nl); ++cc) {
-                    const long long ro = vb + (long long)(ub + cc) * a.out_su;
-                    TO* row = out + ro;
-                    if (a.acc) {
-                        const double* arow = a.acc + ro;
-                        for (int l = lo + t; l <= hi; l += kNT) row[l] = (TO)(arow[l] + (double)buf[l * PR + cc] * sc);
-                    } else {
-                        for (int l = lo + t; l <= hi; l += kNT) row[l] = (TO)((double)buf[l * PR + cc] * sc);
-                    }
-                }
-            } else if (c < nl) {
-                const long long o = vb + (long long)(ub + c) * a.out_su + (long long)(lo + slot) * a.out_sl;
-                TO* p = out + o;
-                const double* q = a.acc ? a.acc + o : nullptr;
-                const long long step = (long long)P * a.out_sl;
-                for (int l = lo + slot; l <= hi; l += P) {
-                    const double x = (double)buf[l * PR + c] * sc;
-                    *p = (TO)(q ? *q + x : x);
-                    p += step;
-                    if (q) q += step;
-                }
-            }
-        }
-        __syncthreads();
+        fast_tile<T, T, T, M, CONTIG, KIND, KIND2>(s_in, s_out, *as, tb, ez_s, buf, red, tile - s_first, s_ntx, t,
+                                                   c, slot);
     }
+}
+
+// Shared memory of the batched kernel: the persistent kernel's plus one pass
+// descriptor.
+template <int M, bool FUSED>
+constexpr size_t batch_smem_bytes() {
+    return ((SmemLayout<double, M, FUSED>::total + 15) & ~size_t(15)) + sizeof(PassArgs);
 }
 
 }  // namespace fast

@@ -95,5 +95,58 @@ int launch_fast_kind(bool contig, int kind, int kind2, const void* in, void* out
     return (int)cudaErrorInvalidValue;
 }
 
+// One group of a batched pass (FP64): the members' tiles are split into
+// contiguous ranges over as many CTAs as fit the device.
+template <int M, bool CONTIG, int KIND, int K2>
+int launch_batch_one(const FastBatchArgs& g, const LineTables<double>& tb, cudaStream_t stream) {
+    auto kern = fast_batch_pass<M, CONTIG, KIND, K2>;
+    constexpr size_t smem = batch_smem_bytes<M, (K2 >= 0)>();
+    static std::atomic<int> ctas_per_sm{0};
+    int cps = ctas_per_sm.load(std::memory_order_relaxed);
+    if (cps == 0) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cps, kern, kNT, smem);
+        if (e != cudaSuccess) return (int)e;
+        if (cps < 1) cps = 1;
+        ctas_per_sm.store(cps, std::memory_order_relaxed);
+    }
+    if (g.ntiles <= 0) return 0;
+    const long long cap = (long long)cps * device_sm_count();
+    const int grid = (int)(g.ntiles < cap ? g.ntiles : cap);
+    kern<<<grid, kNT, smem, stream>>>(g, tb);
+    return (int)cudaGetLastError();
+}
+
+template <int M>
+int launch_fast_batch_kind(bool contig, int kind, int kind2, const FastBatchArgs& g, const LineTables<double>& tb,
+                           cudaStream_t stream) {
+#define CHZ_SINGLE(K)                                                        \
+    case K:                                                                  \
+        if (contig) return launch_batch_one<M, true, K, -1>(g, tb, stream);  \
+        return launch_batch_one<M, false, K, -1>(g, tb, stream);
+    if (kind2 < 0) {
+        switch (kind) {
+            CHZ_SINGLE(kDCT1)
+            CHZ_SINGLE(kDCT2)
+            CHZ_SINGLE(kDCT3)
+            CHZ_SINGLE(kDST1)
+            CHZ_SINGLE(kDST2)
+            CHZ_SINGLE(kDST3)
+            CHZ_SINGLE(kR2C)
+            CHZ_SINGLE(kC2R)
+            default: return (int)cudaErrorInvalidValue;
+        }
+    }
+#undef CHZ_SINGLE
+    if (contig) return (int)cudaErrorInvalidValue;
+    if (kind == kR2C && kind2 == kC2R) return launch_batch_one<M, false, kR2C, kC2R>(g, tb, stream);
+    if (kind == kDST1 && kind2 == kDST1) return launch_batch_one<M, false, kDST1, kDST1>(g, tb, stream);
+    if (kind == kDST3 && kind2 == kDST2) return launch_batch_one<M, false, kDST3, kDST2>(g, tb, stream);
+    if (kind == kDCT1 && kind2 == kDCT1) return launch_batch_one<M, false, kDCT1, kDCT1>(g, tb, stream);
+    if (kind == kDCT3 && kind2 == kDCT2) return launch_batch_one<M, false, kDCT3, kDCT2>(g, tb, stream);
+    return (int)cudaErrorInvalidValue;
+}
+
 }  // namespace fast
 }  // namespace chz

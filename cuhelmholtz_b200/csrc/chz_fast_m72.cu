@@ -1,4 +1,4 @@
-// Instantiation of the register-resident line kernels for N = 144 (M = 72), FP64.
+// Instantiation of the register-resident line kernels for N = 144 (M = 72), FP64, single and batched.
 #include "chz_fast_launch.cuh"
 
 namespace chz {
@@ -6,5 +6,7 @@ namespace fast {
 template int launch_fast_kind<double, double, double, 72>(bool, int, int, const void*, void*, const PassArgs&,
                                                            const LineTables<double>&, int, cudaStream_t,
                                                            const char*);
+template int launch_fast_batch_kind<72>(bool, int, int, const FastBatchArgs&, const LineTables<double>&,
+                                         cudaStream_t);
 }  // namespace fast
 }  // namespace chz

@@ -135,6 +135,43 @@ LineGeom line_geometry(int N, int is_double, bool contig);
 // `max_smem` bytes.
 LineGeom line_geometry_target(int N, int is_double, bool contig, int target, size_t max_smem);
 
+// Array pointers of one problem of a batched solve, set at every call.
+struct BatchPtrs {
+    double* f;
+    const double* face[6];  // bcl, bcr, bcb, bct, bcf, bce
+};
+
+// One problem of a group of a batched pass that a register-resident kernel
+// runs (every member of a group has the same line length and kinds).
+struct BatchMember {
+    PassArgs a;        // the problem's pass; f and the Neumann faces come from ptrs[prob]
+    int prob;          // problem index (into the pointer table)
+    int ntx;           // tiles along u (the kernel's W lines each)
+    int in_user;       // input: the problem's f (else its work array at ws_off)
+    int out_user;      // output: the problem's f
+    long long ws_off;  // offset of the problem's work array in ws (doubles)
+};
+
+// A group launch: tiles 0 .. ntiles - 1 over the members, member m owning
+// tiles start[m] .. start[m + 1] - 1.
+struct FastBatchArgs {
+    const BatchMember* members;
+    const int* start;
+    int count;
+    int ntiles;
+    const BatchPtrs* ptrs;
+    double* ws;
+};
+
+// Register-resident kernels: lengths they take (FP64 every power of two 16 ..
+// 512 and the mixed lengths with a radix plan; FP32 the powers of two), lines
+// per tile of the persistent kernel at a half length M (0: none), and the
+// launch of one batched group (FP64).
+bool fast_path_supported(int M, bool is_double);
+int fast_lines_per_tile(int M);
+int launch_fast_batch(bool contig, int kind, int kind2, const FastBatchArgs& g, const LineTables<double>& tb,
+                      cudaStream_t stream);
+
 // Launchers (return cudaError_t as int).
 enum IoType { kIoF64 = 0, kIoF32 = 1 };
 int launch_line_pass(int is_double, int in_type, int out_type, bool contig, const void* in,

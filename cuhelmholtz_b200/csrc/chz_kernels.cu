@@ -26,6 +26,7 @@
 #include "chz_internal.h"
 
 #include "chz_generic.cuh"
+#include "chz_fast.cuh"
 
 namespace chz {
 
@@ -288,6 +289,9 @@ namespace fast {
 template <typename T, typename TI, typename TO, int M>
 int launch_fast_kind(bool contig, int kind, int kind2, const void* in, void* out, const PassArgs& a,
                      const LineTables<T>& tb, int nv, cudaStream_t stream, const char* label);
+template <int M>
+int launch_fast_batch_kind(bool contig, int kind, int kind2, const FastBatchArgs& g, const LineTables<double>& tb,
+                           cudaStream_t stream);
 
 int device_sm_count() {
     static std::atomic<int> cached[64];
@@ -339,6 +343,30 @@ static int launch_fast_t(bool contig, const void* in, void* out, const PassArgs&
     }
     return (int)cudaErrorInvalidValue;
 #undef CHZ_M
+}
+
+#define CHZ_FAST_LENGTHS(X) \
+    X(12) X(16) X(20) X(24) X(28) X(32) X(40) X(48) X(56) X(64) X(72) X(80) X(96) X(128) X(160) X(192) X(256) X(512)
+
+int fast_lines_per_tile(int M) {
+    switch (M) {
+#define CHZ_W(MM) \
+    case MM: return fast::Cfg<MM>::W;
+        CHZ_FAST_LENGTHS(CHZ_W)
+#undef CHZ_W
+        default: return 0;
+    }
+}
+
+int launch_fast_batch(bool contig, int kind, int kind2, const FastBatchArgs& g, const LineTables<double>& t,
+                      cudaStream_t stream) {
+    switch (t.M) {
+#define CHZ_B(MM) \
+    case MM: return fast::launch_fast_batch_kind<MM>(contig, kind, kind2, g, t, stream);
+        CHZ_FAST_LENGTHS(CHZ_B)
+#undef CHZ_B
+        default: return (int)cudaErrorInvalidValue;
+    }
 }
 
 namespace tma {

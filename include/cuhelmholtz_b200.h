@@ -159,8 +159,12 @@ int chz_helmholtz_adjoint(double left, double right, int nx, int xbc,
  *      passes of every problem, pass by pass, then each problem's periodic
  *      planes; an item waits -- bounded -- for its problem's previous pass),
  *      with the reset of its counters;
- *   1: one launch per pass over all problems, then one for the periodic
- *      planes.
+ *   1: per pass, one launch of the register-resident line kernel for each
+ *      group of problems with the same line length and kinds (the lengths
+ *      with a register radix plan: powers of two 32..1024 and the mixed
+ *      N = 24..384 listed under chz_set_kernel_family), then one launch of
+ *      the shared-memory mixed-radix kernel over the other problems; then one
+ *      launch for the periodic planes.
  * The plan times both at creation and keeps the faster
  * (chz_batch_plan_launch).  A wait that runs out is reported by
  * chz_stream_status.
@@ -212,6 +216,11 @@ int chz_batch_plan_launch(const chz_batch_plan* plan, int* mode, float* ms);
  * default, times both).  Returns the previous setting, or -2 for an unknown
  * form. */
 int chz_batch_set_launch_mode(int mode);
+
+/* Kernel launches one chz_batch_solve of this plan replays (1 in the
+ * persistent form; the groups, leftover launches and periodic-plane launch in
+ * the per-pass form); CHZ_ERROR_INVALID_VALUE (negative) for a NULL plan. */
+int chz_batch_plan_kernels(const chz_batch_plan* plan);
 
 /* Helmholtz solve with FP32 transforms and FP64 iterative refinement.
  * u0 = S32(b); then up to max_corrections times: r = b - A u in FP64 (the
@@ -304,12 +313,14 @@ int chz_trace_enable(int on);
 int chz_trace_collect(char* buf, size_t len);
 
 /* Kernel family: 0 (default) uses the TMA-pipelined kernel for the strided
- * (y, z) passes of N = 128, 256, 512, the register-resident line kernels for
- * the other passes of lengths N = 32..1024 that are powers of two, and the
- * shared-memory mixed-radix kernel elsewhere; 1 uses the mixed-radix kernel
- * for every pass; 2 is family 0 without the TMA kernel (all are checked
- * against the same oracle).  Returns the previous setting, or -1 for an
- * unknown family. */
+ * (y, z) passes of N = 128, 192, 256, 320, 512 (FP64; 128, 256, 512 in FP32),
+ * the register-resident line kernels for the other passes of lengths
+ * N = 32..1024 that are powers of two and, in FP64, of the mixed lengths
+ * N = 24, 40, 48, 56, 80, 96, 112, 144, 160, 192, 320, 384 (radix plans with
+ * factors 3, 5, 7), and the shared-memory mixed-radix kernel elsewhere; 1
+ * uses the mixed-radix kernel for every pass; 2 is family 0 without the TMA
+ * kernel (all are checked against the same oracle).  Returns the previous
+ * setting, or -1 for an unknown family. */
 int chz_set_kernel_family(int family);
 
 /* Flags raised by the kernels' bounded waits since the last reset (0 when no
