@@ -27,6 +27,7 @@
 #include <mutex>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <new>
 #include <vector>
 
@@ -265,6 +266,7 @@ using namespace chz;
 // The problems of one pass that a register-resident kernel takes, grouped
 // by (length, kinds): one launch each.
 struct FastGroup {
+    std::vector<int> probs;   // member problems
     int kind = 0, kind2 = -1;
     chz::LineTables<double> tb{};
     chz::BatchMember* members_d = nullptr;
@@ -310,6 +312,15 @@ struct chz_batch_plan {
     int left_count[kPasses] = {};
     int left_tiles[kPasses] = {};
     size_t left_smem[kPasses] = {};
+    // The launches of the per-pass form ("units": the groups of pass q, then
+    // its leftover launch) run as a graph of branches: a unit waits only for
+    // the units of pass q - 1 that hold one of its problems (deps), so
+    // independent launches run at once.
+    std::vector<std::vector<int>> deps[kPasses];
+    std::vector<cudaEvent_t> done[kPasses];
+    std::vector<cudaStream_t> branch;
+    std::vector<cudaEvent_t> join;      // one per branch stream: its last work, joined into the caller's stream
+    cudaEvent_t fork = nullptr;
 };
 
 namespace {
@@ -328,7 +339,11 @@ void free_plan(chz_batch_plan* p) {
         if (p->left_items_d[q]) cudaFree(p->left_items_d[q]);
         if (p->left_start_d[q]) cudaFree(p->left_start_d[q]);
         if (p->left_prob_d[q]) cudaFree(p->left_prob_d[q]);
+        for (cudaEvent_t ev : p->done[q]) cudaEventDestroy(ev);
     }
+    for (cudaStream_t st : p->branch) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : p->join) cudaEventDestroy(ev);
+    if (p->fork) cudaEventDestroy(p->fork);
     if (p->fix_d) cudaFree(p->fix_d);
     if (p->ptrs_d) cudaFree(p->ptrs_d);
     if (p->ptrs_h) cudaFreeHost(p->ptrs_h);
@@ -431,13 +446,13 @@ cudaError_t launch_pass(chz_batch_plan* p, int q, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-// Pass q as the per-pass form runs it: one register-resident launch per
-// group, then the generic kernel over the leftovers.
-cudaError_t launch_pass_grouped(chz_batch_plan* p, int q, cudaStream_t s) {
-    for (const FastGroup& g : p->groups[q]) {
+// Unit u of pass q in the per-pass form: register-resident group u, or (u ==
+// the number of groups) the generic kernel over the leftovers.
+cudaError_t launch_unit(chz_batch_plan* p, int q, int u, cudaStream_t s) {
+    if (u < (int)p->groups[q].size()) {
+        const FastGroup& g = p->groups[q][u];
         FastBatchArgs A{g.members_d, g.start_d, g.count, g.ntiles, p->ptrs_d, p->ws};
-        const int rc = launch_fast_batch(p->contig[q], g.kind, g.kind2, A, g.tb, s);
-        if (rc != 0) return (cudaError_t)rc;
+        return (cudaError_t)launch_fast_batch(p->contig[q], g.kind, g.kind2, A, g.tb, s);
     }
     if (p->left_count[q] == 0 || p->left_tiles[q] == 0) return cudaSuccess;
     if (p->contig[q])
@@ -447,6 +462,81 @@ cudaError_t launch_pass_grouped(chz_batch_plan* p, int q, cudaStream_t s) {
         batch_pass<false><<<p->left_tiles[q], kThreads, p->left_smem[q], s>>>(
             p->left_items_d[q], p->left_start_d[q], p->left_count[q], p->ptrs_d, p->ws, p->left_prob_d[q]);
     return cudaGetLastError();
+}
+
+int units_of(const chz_batch_plan* p, int q) {
+    return (int)p->groups[q].size() + ((p->left_count[q] > 0 && p->left_tiles[q] > 0) ? 1 : 0);
+}
+
+constexpr int kBranches = 16;   // side streams of the per-pass form
+
+// The per-pass form's dependencies: unit u of pass q waits for the units of
+// pass q - 1 that hold one of its problems; plus the branch streams and one
+// event per unit.
+cudaError_t build_branches(chz_batch_plan* p) {
+    std::vector<int> unit_of[kPasses];
+    for (int q = 0; q < kPasses; ++q) {
+        unit_of[q].assign(p->count, -1);
+        // members of each group, read back from the host-side grouping
+        for (int u = 0; u < (int)p->groups[q].size(); ++u)
+            for (int i : p->groups[q][u].probs) unit_of[q][i] = u;
+        for (int i = 0; i < p->count; ++i)
+            if (unit_of[q][i] < 0) unit_of[q][i] = (int)p->groups[q].size();   // the leftover unit
+    }
+    for (int q = 0; q < kPasses; ++q) {
+        const int nu = units_of(p, q);
+        p->deps[q].assign(nu, {});
+        if (q > 0) {
+            std::vector<std::vector<char>> seen(nu, std::vector<char>(units_of(p, q - 1) + 1, 0));
+            for (int i = 0; i < p->count; ++i) {
+                const int u = unit_of[q][i], d = unit_of[q - 1][i];
+                if (u < nu && d < units_of(p, q - 1) && !seen[u][d]) {
+                    seen[u][d] = 1;
+                    p->deps[q][u].push_back(d);
+                }
+            }
+        }
+        p->done[q].assign(nu, nullptr);
+        for (int u = 0; u < nu; ++u) {
+            const cudaError_t e = cudaEventCreateWithFlags(&p->done[q][u], cudaEventDisableTiming);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    cudaError_t e = cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming);
+    for (int k = 0; k < kBranches && e == cudaSuccess; ++k) {
+        cudaStream_t st = nullptr;
+        e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        if (e == cudaSuccess) p->branch.push_back(st);
+        cudaEvent_t ev = nullptr;
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e == cudaSuccess) p->join.push_back(ev);
+    }
+    return e;
+}
+
+// The five passes of the per-pass form on the branch streams, forked from and
+// joined back into `s`.
+cudaError_t launch_passes_grouped(chz_batch_plan* p, cudaStream_t s) {
+    cudaError_t e = cudaEventRecord(p->fork, s);
+    int k = 0;
+    for (int q = 0; q < kPasses && e == cudaSuccess; ++q) {
+        for (int u = 0; u < units_of(p, q) && e == cudaSuccess; ++u) {
+            cudaStream_t st = p->branch[(k++) % p->branch.size()];
+            if (q == 0) e = cudaStreamWaitEvent(st, p->fork, 0);
+            for (int d : p->deps[q][u])
+                if (e == cudaSuccess) e = cudaStreamWaitEvent(st, p->done[q - 1][d], 0);
+            if (e == cudaSuccess) e = launch_unit(p, q, u, st);
+            if (e == cudaSuccess) e = cudaEventRecord(p->done[q][u], st);
+        }
+    }
+    // every branch stream that took work joins back into s (a captured
+    // graph's forks must all be joined)
+    const int used = std::min<int>(k, (int)p->branch.size());
+    for (int b = 0; b < used && e == cudaSuccess; ++b) {
+        e = cudaEventRecord(p->join[b], p->branch[b]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, p->join[b], 0);
+    }
+    return e;
 }
 
 // Splits pass q into register-resident groups (problems whose line length has
@@ -467,6 +557,7 @@ cudaError_t build_groups(chz_batch_plan* p, int q, const std::vector<PassTemplat
         const int M = std::get<0>(kv.first);
         const int W = fast_lines_per_tile(M);
         FastGroup g;
+        g.probs = kv.second;
         g.kind = std::get<1>(kv.first);
         g.kind2 = std::get<2>(kv.first);
         g.tb = items[kv.second[0]].tb;
@@ -645,8 +736,8 @@ cudaError_t prepare_persistent(chz_batch_plan* p) {
 // five pass launches, then the periodic planes.
 int enqueue(chz_batch_plan* p, cudaStream_t s) {
     if (p->mode == 1) {
-        for (int q = 0; q < kPasses; ++q) {
-            const cudaError_t e = launch_pass_grouped(p, q, s);
+        {
+            const cudaError_t e = launch_passes_grouped(p, s);
             if (e != cudaSuccess) return cuda_fail((int)e, "batched pass");
         }
         if (p->periodic) {
@@ -885,6 +976,7 @@ int chz_batch_plan_create(int count, const int* dims, const int* bcs, const doub
         e = upload_pass(p, q, items[q], start[q]);
         if (e == cudaSuccess) e = build_groups(p, q, tmpl[q], items[q]);
     }
+    if (e == cudaSuccess) e = build_branches(p);
     if (e == cudaSuccess) e = cudaMalloc(&p->counters, sizeof(int) * ((size_t)count * kPasses + 1));
     if (e == cudaSuccess) {
         // the problem of every pass tile, in queue order
@@ -1007,8 +1099,7 @@ int chz_batch_plan_kernels(const chz_batch_plan* plan) {
     if (!plan) return fail(CHZ_ERROR_INVALID_VALUE, "NULL plan");
     if (plan->mode == 0) return 1;
     int n = plan->periodic ? 1 : 0;
-    for (int q = 0; q < kPasses; ++q)
-        n += (int)plan->groups[q].size() + ((plan->left_count[q] > 0 && plan->left_tiles[q] > 0) ? 1 : 0);
+    for (int q = 0; q < kPasses; ++q) n += units_of(plan, q);
     return n;
 }
 

@@ -164,13 +164,16 @@ def test_batch_is_one_launch_per_solve():
 
 @pytest.mark.parametrize("mode", [0, 1])
 def test_each_launch_form_matches_single_solves(mode):
-    """Both launch forms (0: persistent work queue; 1: a launch per pass, then
-    the periodic planes) give the single solves' results, periodic axes
+    """Both launch forms (0: persistent work queue; 1: per pass, register-
+    resident launches on groups of problems with the same line length and
+    kinds and the generic kernel on the rest -- here N = 176 -- then the
+    periodic planes) give the single solves' results, periodic axes
     included."""
     probs = [gen.random_problem(nx, ny, nz, xbc, ybc, zbc, lam, seed=970 + i)
              for i, (nx, ny, nz, xbc, ybc, zbc, lam) in enumerate(
                  [(48, 64, 32, 0, 0, 0, -1.0), (96, 40, 56, 1, 0, 3, -4.0), (32, 32, 144, 3, 4, 0, -0.2),
-                  (80, 112, 48, 2, 1, 4, -9.0), (64, 48, 96, 0, 3, 2, -0.6)])]
+                  (80, 112, 48, 2, 1, 4, -9.0), (64, 48, 96, 0, 3, 2, -0.6), (176, 40, 48, 4, 2, 1, -2.5),
+                  (96, 176, 96, 1, 1, 3, -0.8)])]
     prev = api.BatchPlan.set_launch_mode(mode)
     try:
         plan = api.BatchPlan(probs)
@@ -178,6 +181,10 @@ def test_each_launch_form_matches_single_solves(mode):
         api.BatchPlan.set_launch_mode(prev)
     m, ms = plan.launch_mode()
     assert m == mode and ms == [0.0, 0.0]
+    # kernels a solve replays: one persistent launch, or per pass the groups
+    # (x forward alone has 5 (length, kind) groups here) plus the leftover
+    # launch, then the periodic planes
+    assert plan.kernels() == 1 if mode == 0 else plan.kernels() >= 5 + 5 + 1
     for _ in range(2):      # two graph replays, each on fresh copies of the right-hand sides
         fs, faces = zip(*[_dev(p) for p in probs])
         plan.solve(list(fs), list(faces))

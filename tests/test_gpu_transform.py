@@ -60,11 +60,14 @@ def kernel_family(request):
     api.set_kernel_family(prev)
 
 
-@pytest.mark.parametrize("n", [4, 6, 10, 16, 24, 32, 40, 56, 64, 88, 96, 104, 128, 160, 256, 512, 1024])
+@pytest.mark.parametrize("n", [4, 6, 10, 16, 24, 32, 40, 48, 56, 64, 80, 88, 96, 104, 112, 128, 144, 160, 192,
+                               256, 320, 384, 512, 1024])
 def test_every_kind_per_length(n, kernel_family):
     """Each kind on each axis at one line length (radices 2..13, odd N/2), with
-    the register-resident kernels (N = 32..1024, powers of two) and with the
-    generic kernel for every length."""
+    the register-resident kernels (N = 32..1024, powers of two, and the mixed
+    radix plans N = 24, 40, 48, 56, 80, 96, 112, 144, 160, 192, 320, 384; the
+    TMA-pipelined strided pass at 192 and 320) and with the generic kernel for
+    every length."""
     rng = np.random.default_rng(n)
     other = 6
     for kind in range(8):
