@@ -370,13 +370,15 @@ __device__ __forceinline__ C2<T> inv_spectrum_v(int kind, const V& X, int k, int
                                                 const LineTables<T>& tb) {
     if constexpr (V::kPair) {
         if (kind == kC2R && k != 0 && k != M) return X.pair(2 * k);
+        // the odd neighbour x[2k - 1] alone (8 bytes): its pair partner
+        // x[2k - 2] is not needed
         if (kind == kDCT1 && k != 0 && k != M) {
-            const C2<T> p1 = X.pair(2 * k), p0 = X.pair(2 * k - 2);
-            return mk<T>(p1.x, p0.y - p1.y);
+            const C2<T> p1 = X.pair(2 * k);
+            return mk<T>(p1.x, X(2 * k - 1) - p1.y);
         }
         if (kind == kDST1 && k != 0 && k != M) {
-            const C2<T> p1 = X.pair(2 * k), p0 = X.pair(2 * k - 2);
-            return mk<T>(p1.y - p0.y, -p1.x);
+            const C2<T> p1 = X.pair(2 * k);
+            return mk<T>(p1.y - X(2 * k - 1), -p1.x);
         }
     }
     switch (kind) {

@@ -361,7 +361,7 @@ __device__ __forceinline__ void transform_lines_v(const V& X, T* buf, T* red, in
     // entries x[2n + 1] the pre step reads for this thread's inputs n, so the
     // partial sum is published only after those reads (no store between them
     // lets the compiler load each entry once)
-    T acc = T(0);
+    T acc = T(0), S = T(0);
     if constexpr (KIND == kDCT1) {
 #pragma unroll
         for (int q = 0; q < M / P; ++q) {
@@ -377,6 +377,14 @@ __device__ __forceinline__ void transform_lines_v(const V& X, T* buf, T* red, in
         for (int k = 0; k < VPT; ++k) v[k] = pre_value<T, KIND, M>(X, BF::in_idx(slot, 0, k), tb);
         if constexpr (KIND == kDCT1) red[slot * W + c] = acc;
         CF::sync();
+        // DCT1: the line's odd-entry sum, by the thread of slot 0, while the
+        // other warps run stage 0 (the partials stay until the next pre step)
+        if constexpr (KIND == kDCT1) {
+            if (slot == 0) {
+#pragma unroll
+                for (int q = 0; q < P; ++q) S += red[q * W + c];
+            }
+        }
         stage_compute<T, M, 0>(v, slot, tb.twM);
     }
 
@@ -456,13 +464,6 @@ __device__ __forceinline__ void transform_lines_v(const V& X, T* buf, T* red, in
     } else if constexpr (KIND == kDCT1 || KIND == kDST1) {
         // v[n] = Re conj(Z[n/2]) (n even), Im conj(Z[n/2]) (n odd); pairs (k, N-k)
         T outs[2 * VPT];
-        T S = T(0);
-        if constexpr (KIND == kDCT1) {
-            if (slot == 0) {
-#pragma unroll
-                for (int q = 0; q < P; ++q) S += red[q * W + c];
-            }
-        }
         T extra = T(0);  // out[N] (DCT1, m = 0)
 #pragma unroll
         for (int b = 0; b < LB::B; ++b)

@@ -351,11 +351,14 @@ struct TmaSmem {
     __host__ __device__ static size_t total(int rows_buf) { return abort(rows_buf) + 16; }
 };
 
-// One CTA per SM asked of the compiler for the power-of-two lengths (the
-// pipeline's shared memory allows no more at N = 512), two for the mixed ones
-// (smaller tiles, fewer compute warps a CTA).
+// CTAs per SM asked of the compiler: one at N = 512 (the pipeline's shared
+// memory allows no more), four at N = 128 (three warps a CTA, 50 KB), two
+// elsewhere.  Registers are allocated per SM sub-partition: two CTAs of five
+// warps (or four of three) put three warps on some sub-partitions, so a
+// thread may hold at most 168 (3 x 32 x 168 <= 16384), which these block
+// counts ask of the compiler.
 template <int M>
-constexpr int tma_min_ctas() { return (M & (M - 1)) == 0 ? 1 : 2; }
+constexpr int tma_min_ctas() { return M >= 256 ? 1 : (M <= 64 ? 4 : 2); }
 
 template <typename T, int M, int KIND, int KIND2>
 __global__ void __launch_bounds__(TCfg<T, M>::NT + 32, tma_min_ctas<M>())
