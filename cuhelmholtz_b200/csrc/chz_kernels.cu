@@ -270,7 +270,8 @@ static int launch_typed(const void* in, void* out, const PassArgs& a, const Devi
 }
 
 // Power-of-two half lengths 16..512 use the register-resident kernels (FP64
-// and FP32); the mixed lengths with a register radix plan use them in FP64.
+// and FP32); the mixed lengths with a register radix plan use them in FP64,
+// and in FP32 at N = 192, 320, 384 (the others: the generic kernel).
 static bool fast_mixed_length(int M) {
     switch (M) {
         case 12: case 20: case 24: case 28: case 40: case 48: case 56: case 72: case 80: case 96: case 160:
@@ -282,7 +283,8 @@ static bool fast_mixed_length(int M) {
 }
 bool fast_path_supported(int M, bool is_double) {
     if (M >= 16 && M <= 512 && (M & (M - 1)) == 0) return true;
-    return is_double && fast_mixed_length(M);
+    if (!is_double) return M == 96 || M == 160 || M == 192;
+    return fast_mixed_length(M);
 }
 
 namespace fast {
@@ -323,8 +325,14 @@ static int launch_fast_t(bool contig, const void* in, void* out, const PassArgs&
         CHZ_M(512);
         default: break;
     }
-    if constexpr (std::is_same<T, double>::value && std::is_same<TI, double>::value &&
-                  std::is_same<TO, double>::value) {
+    if constexpr (std::is_same<T, float>::value) {
+        switch (tb.M) {
+            CHZ_M(96);
+            CHZ_M(160);
+            CHZ_M(192);
+            default: return (int)cudaErrorInvalidValue;
+        }
+    } else {
         switch (tb.M) {
             CHZ_M(12);
             CHZ_M(20);
@@ -389,12 +397,10 @@ static int try_tma(const void* in, void* out, const PassArgs& a, const DeviceLin
         case 256: return tma::launch_tma_kind<T, 256>(a.kind, a.kind2, in, out, a, t, nv, stream, label);
         default: break;
     }
-    if constexpr (std::is_same<T, double>::value) {
-        switch (tb.M) {
-            case 96: return tma::launch_tma_kind<T, 96>(a.kind, a.kind2, in, out, a, t, nv, stream, label);
-            case 160: return tma::launch_tma_kind<T, 160>(a.kind, a.kind2, in, out, a, t, nv, stream, label);
-            default: break;
-        }
+    switch (tb.M) {
+        case 96: return tma::launch_tma_kind<T, 96>(a.kind, a.kind2, in, out, a, t, nv, stream, label);
+        case 160: return tma::launch_tma_kind<T, 160>(a.kind, a.kind2, in, out, a, t, nv, stream, label);
+        default: break;
     }
     return -1;
 }

@@ -357,11 +357,15 @@ struct TmaSmem {
 // warps (or four of three) put three warps on some sub-partitions, so a
 // thread may hold at most 168 (3 x 32 x 168 <= 16384), which these block
 // counts ask of the compiler.
-template <int M>
-constexpr int tma_min_ctas() { return M >= 256 ? 1 : (M <= 64 ? 4 : 2); }
+// The FP32 pass at N = 320 (nine warps, 20 values a thread) keeps one CTA
+// per SM: two would leave it 113 registers and spill.
+template <typename T, int M>
+constexpr int tma_min_ctas() {
+    return M >= 256 ? 1 : (M <= 64 ? 4 : ((sizeof(T) == 4 && M == 160) ? 1 : 2));
+}
 
 template <typename T, int M, int KIND, int KIND2>
-__global__ void __launch_bounds__(TCfg<T, M>::NT + 32, tma_min_ctas<M>())
+__global__ void __launch_bounds__(TCfg<T, M>::NT + 32, tma_min_ctas<T, M>())
 tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUtensorMap stmap, PassArgs a,
          LineTables<T> tg, TmaGeom g, int ntx, int ntiles, int* flags, long long wait_limit) {
     using CF = TCfg<T, M>;

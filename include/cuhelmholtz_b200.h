@@ -313,11 +313,11 @@ int chz_trace_enable(int on);
 int chz_trace_collect(char* buf, size_t len);
 
 /* Kernel family: 0 (default) uses the TMA-pipelined kernel for the strided
- * (y, z) passes of N = 128, 192, 256, 320, 512 (FP64; 128, 256, 512 in FP32),
- * the register-resident line kernels for the other passes of lengths
- * N = 32..1024 that are powers of two and, in FP64, of the mixed lengths
- * N = 24, 40, 48, 56, 80, 96, 112, 144, 160, 192, 320, 384 (radix plans with
- * factors 3, 5, 7), and the shared-memory mixed-radix kernel elsewhere; 1
+ * (y, z) passes of N = 128, 192, 256, 320, 512, the register-resident line
+ * kernels for the other passes of lengths N = 32..1024 that are powers of two
+ * and of the mixed lengths N = 24, 40, 48, 56, 80, 96, 112, 144, 160, 192,
+ * 320, 384 (radix plans with factors 3, 5, 7; in FP32 only 192, 320, 384),
+ * and the shared-memory mixed-radix kernel elsewhere; 1
  * uses the mixed-radix kernel for every pass; 2 is family 0 without the TMA
  * kernel (all are checked against the same oracle).  Returns the previous
  * setting, or -1 for an unknown family. */
