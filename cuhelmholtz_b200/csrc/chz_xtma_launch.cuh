@@ -35,14 +35,15 @@ int launch_one(const double* in, double* out, const PassArgs& a, const LineTable
                cudaStream_t stream, const char* label) {
     using CF = XCfg<M>;
     using SL = XSmem<double, M>;
-    constexpr int W = CF::W, N = CF::N;
+    constexpr int W = CF::W, TW = CF::TW, N = CF::N;
     constexpr int LO = fast::InWin<KIND, N>::lo, HI = fast::InWin<KIND, N>::hi;
     if ((long long)SL::total > (long long)tma::max_optin_smem()) return -1;
     XGeom g{};
     CUtensorMap ldmap, stmap;
     std::memset(&ldmap, 0, sizeof(ldmap));
     std::memset(&stmap, 0, sizeof(stmap));
-    const unsigned box[3] = {16u, 16u, 1u};
+    // a box is one 16-entry block of the W lines of a compute group
+    const unsigned box[3] = {16u, (unsigned)W, 1u};
     // the maps start at the pass's first plane v0 (16-byte aligned: whole
     // planes of 16-byte-aligned rows); a caller may hand a base moved back by
     // planes it never addresses (the slab solve), and a tensor map's base must
@@ -57,8 +58,9 @@ int launch_one(const double* in, double* out, const PassArgs& a, const LineTable
         if (!tma::encode_map_swz(&ldmap, in + (long long)a.v0 * a.in_sv, dims, strides, box)) return -1;
     } else {
         // whole rows of the span, row-major: the kind's input window inside a
-        // row, and the W rows (plus the span's misalignment) inside a stage
-        if (HI > a.in_su - 1 || a.in_sv < a.in_su * (a.u0 + a.nu) || W * a.in_su + 2 > CF::BUF) return -1;
+        // row, and a group's W rows (plus the span's misalignment) inside its
+        // region of a stage
+        if (HI > a.in_su - 1 || a.in_sv < a.in_su * (a.u0 + a.nu) || W * a.in_su + 2 > CF::GBUF) return -1;
     }
     if (STM == kStTensor) {
         g.st_blk0 = a.st_lo >> 4;
@@ -73,7 +75,7 @@ int launch_one(const double* in, double* out, const PassArgs& a, const LineTable
         // every entry of it), the W rows inside a stage, 8-byte-aligned rows
         int o0, o1;
         kind_out_window(KIND, N, o0, o1);
-        if (o1 > a.out_su - 1 || a.st_lo < 0 || a.st_hi > a.out_su - 1 || W * a.out_su + 2 > CF::BUF ||
+        if (o1 > a.out_su - 1 || a.st_lo < 0 || a.st_hi > a.out_su - 1 || W * a.out_su + 2 > CF::GBUF ||
             (reinterpret_cast<uintptr_t>(out) & 7))
             return -1;
     }
@@ -91,7 +93,7 @@ int launch_one(const double* in, double* out, const PassArgs& a, const LineTable
         if (cps < 1) return -1;
         cps_cached.store(cps, std::memory_order_relaxed);
     }
-    const int ntx = (a.nu + W - 1) / W;
+    const int ntx = (a.nu + TW - 1) / TW;
     const long long ntiles = (long long)ntx * nv;
     if (ntiles <= 0) return 0;
     if (ntiles > 0x7fffffffLL) return -1;
