@@ -595,9 +595,16 @@ __device__ __forceinline__ void load_tile(T* buf, const TI* __restrict__ in, con
     asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
 
+// Contiguous FP32 passes with an FP64 output (the refinement's x inverse):
+// the rows an accumulated output adds to are staged in shared memory by
+// cp.async while the tile is transformed.
+template <typename T, typename TO, bool CONTIG>
+constexpr bool acc_staged() { return CONTIG && sizeof(T) == 4 && sizeof(TO) == 8; }
+
 // Shared-memory footprint of one CTA (bytes): tile buffer, DCT1 partials,
-// the line tables and, for the fused pass, the z eigenvalue table.
-template <typename T, int M, bool FUSED>
+// the line tables, for the fused pass the z eigenvalue table and, with ACC,
+// the staged rows of an accumulated output (W rows of N + 2 FP64 values).
+template <typename T, int M, bool FUSED, bool ACC = false>
 struct SmemLayout {
     using CF = Cfg<M>;
     static constexpr size_t buf = 0;
@@ -607,7 +614,8 @@ struct SmemLayout {
     static constexpr size_t tw4N = twN + sizeof(C2<T>) * (M + 1);
     static constexpr size_t inv4sin = tw4N + sizeof(C2<T>) * (M + 1);
     static constexpr size_t ez = (inv4sin + sizeof(T) * (M + 1) + 15) & ~size_t(15);
-    static constexpr size_t total = ez + (FUSED ? sizeof(double) * (2 * M + 2) : 0);
+    static constexpr size_t accb = (ez + (FUSED ? sizeof(double) * (2 * M + 2) : 0) + 15) & ~size_t(15);
+    static constexpr size_t total = accb + (ACC ? sizeof(double) * CF::W * (2 * M + 2) : 0);
 };
 
 // Four CTAs per SM (128 registers a thread); three for plans of more than 16
@@ -621,15 +629,32 @@ constexpr int fast_min_ctas() { return Plan<M>::V > kR ? 3 : 4; }
 template <typename T, typename TI, typename TO, int M, bool CONTIG, int KIND, int KIND2>
 __device__ __forceinline__ void fast_tile(const TI* in, TO* out, const PassArgs& a, const LineTables<T>& tb,
                                           const double* ez_s, T* buf, T* red, int tile, int ntx, int t, int c,
-                                          int slot) {
+                                          int slot, double* accb = nullptr) {
     using CF = Cfg<M>;
     constexpr int W = CF::W, PR = CF::PR, P = CF::P, N = CF::N;
+    constexpr bool ACCS = acc_staged<T, TO, CONTIG>();
     const int tx = tile % ntx;
     const int v = a.v0 + tile / ntx;
     const int ub = a.u0 + tx * W;
     const int nl = min(W, a.u0 + a.nu - ub);
     load_tile<T, TI, M, CONTIG, KIND>(buf, in, a, ub, nl, v, t, c, slot);
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    // the rows an accumulated output adds to: a second copy group, waited
+    // for only before the store, so its latency overlaps the transform
+    bool staged = false;
+    if constexpr (ACCS) {
+        if (a.acc) {
+            const long long vb = (long long)v * a.out_sv;
+            for (int cc = 0; cc < nl; ++cc) {
+                const double* arow = a.acc + vb + (long long)(ub + cc) * a.out_su;
+                for (int l = a.st_lo + t; l <= a.st_hi; l += kNT)
+                    cp_async_elem<8>(accb + cc * (N + 2) + l, arow + l, true);
+            }
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+            staged = true;
+        }
+    }
+    if (staged) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    else asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
 
     if (CONTIG && a.has_bc) {
@@ -691,8 +716,20 @@ __device__ __forceinline__ void fast_tile(const TI* in, TO* out, const PassArgs&
             // loads overlap instead of one latency per row
             constexpr int NI = (N + 2 + kNT - 1) / kNT;
             bool done = false;
+            if constexpr (ACCS) {
+                if (staged) {
+                    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+                    __syncthreads();
+                    for (int cc = 0; cc < nl; ++cc) {
+                        TO* row = out + vb + (long long)(ub + cc) * a.out_su;
+                        const double* ar = accb + cc * (N + 2);
+                        for (int l = lo + t; l <= hi; l += kNT) row[l] = (TO)(ar[l] + (double)buf[l * PR + cc] * sc);
+                    }
+                    done = true;
+                }
+            }
             if constexpr (W * NI <= 48) {
-                if (a.acc) {
+                if (a.acc && !done) {
                     double av[W][NI];
 #pragma unroll
                     for (int cc = 0; cc < W; ++cc) {
@@ -746,11 +783,13 @@ template <typename T, typename TI, typename TO, int M, bool CONTIG, int KIND, in
 __global__ void __launch_bounds__(kNT, fast_min_ctas<M>())
 fast_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tg, int ntx, int ntiles) {
     using CF = Cfg<M>;
-    using SL = SmemLayout<T, M, (KIND2 >= 0)>;
+    constexpr bool ACCS = acc_staged<T, TO, CONTIG>();
+    using SL = SmemLayout<T, M, (KIND2 >= 0), ACCS>;
     constexpr int W = CF::W, PR = CF::PR, P = CF::P, N = CF::N;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* buf = reinterpret_cast<T*>(smem_raw + SL::buf);
     T* red = reinterpret_cast<T*>(smem_raw + SL::red);
+    double* accb = ACCS ? reinterpret_cast<double*>(smem_raw + SL::accb) : nullptr;
 
     const int t = threadIdx.x;
     const int c = t % W;
@@ -787,7 +826,7 @@ fast_pass(const TI* in, TO* out, PassArgs a, LineTables<T> tg, int ntx, int ntil
     }
 
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
-        fast_tile<T, TI, TO, M, CONTIG, KIND, KIND2>(in, out, a, tb, ez_s, buf, red, tile, ntx, t, c, slot);
+        fast_tile<T, TI, TO, M, CONTIG, KIND, KIND2>(in, out, a, tb, ez_s, buf, red, tile, ntx, t, c, slot, accb);
 }
 
 // One group of a batched pass (FP64): the members share the length and the

@@ -18,7 +18,7 @@ int launch_one(const void* in, void* out, const PassArgs& a, const LineTables<T>
                cudaStream_t stream, const char* label) {
     using CF = Cfg<M>;
     auto kern = fast_pass<T, TI, TO, M, CONTIG, KIND, K2>;
-    const size_t smem = SmemLayout<T, M, (K2 >= 0)>::total;
+    const size_t smem = SmemLayout<T, M, (K2 >= 0), acc_staged<T, TO, CONTIG>()>::total;
     // per instantiation: opt in to the dynamic shared memory, ask how many CTAs fit
     static std::atomic<int> ctas_per_sm{0};
     int cps = ctas_per_sm.load(std::memory_order_relaxed);
