@@ -177,6 +177,49 @@ __device__ __forceinline__ int paired_slot(int t) {
     return w == 0 ? (P / 2) * h : (h ? P - w : w);
 }
 
+// Pair (m, M - m) of the fused R2C / division / C2R pass, from Z[m] = zk,
+// Z[M - m] = zm: the R2C split gives X[m] and X[M - m] (w^(M-m) = -conj w^m),
+// each is divided by its eigenvalue, and the C2R pre step gives the inverse
+// inputs at m (o1) and M - m (o2, the conjugate sums of o1's).  m = 0 pairs
+// bin 0 with the Nyquist bin M (o2 is then not an input).
+template <typename T, int N, typename DSINK>
+__device__ __forceinline__ void split_div_pre(int m, C2<T> zk, C2<T> zm, C2<T>& o1, C2<T>& o2,
+                                              const LineTables<T>& tb, const DSINK& dv) {
+    const C2<T> wk = ldtw<T>(tb.twN + m);
+    if (m != 0 && 2 * m >= dv.dlo && 2 * m + 1 <= dv.dhi && N - 2 * m >= dv.dlo && N - 2 * m + 1 <= dv.dhi) {
+        // The split, the two divisions and the pre step compose into one
+        // real-linear map of (zk, zm).  With s = zk + conj zm,
+        // t = zk - conj zm, w = w^m = wr + i wi, dm, dp the reciprocal
+        // eigenvalues of bins m and M - m: X[m] = (s - i w t) / 2,
+        // X[M - m] = conj(s + i w t) / 2, and the pre step of the divided
+        // pair gives (|w| = 1)
+        //   o1 = ((dm + dp) + (dm - dp) wi) conj zk - i (dm - dp) wr zm
+        //   o2 = ((dm + dp) - (dm - dp) wi) conj zm - i (dm - dp) wr zk.
+        const T dm = (T)dv.eig(2 * m), dp = (T)dv.eig(N - 2 * m);
+        const T sum = dm + dp, dif = dm - dp;
+        const T c1 = sum + dif * wk.y, c2 = sum - dif * wk.y, g = dif * wk.x;
+        o1 = mk<T>(c1 * zk.x + g * zm.y, -(c1 * zk.y + g * zm.x));
+        o2 = mk<T>(c2 * zm.x + g * zk.y, -(c2 * zm.y + g * zk.x));
+        return;
+    }
+    const C2<T> e = cadd<T>(zk, cconj<T>(zm));
+    const C2<T> od = cmul<T>(wk, csub<T>(zk, cconj<T>(zm)));
+    C2<T> a = mk<T>(T(0.5) * (e.x + od.y), T(0.5) * (e.y - od.x));    // X[m]
+    C2<T> b = mk<T>(T(0.5) * (e.x - od.y), T(-0.5) * (e.y + od.x));   // X[M - m]
+    int lb = N - 2 * m;
+    if (m == 0) {
+        a = mk<T>(zk.x + zk.y, T(0));
+        b = mk<T>(zk.x - zk.y, T(0));
+        lb = N;
+    }
+    dv.div_pair(2 * m, a);
+    dv.div_pair(lb, b);
+    const C2<T> e2 = cadd<T>(a, cconj<T>(b));
+    const C2<T> o2c = cmul<T>(cconj<T>(wk), csub<T>(a, cconj<T>(b)));
+    o1 = cconj<T>(cadd<T>(e2, cmul_i<T>(o2c)));
+    o2 = cconj<T>(cadd<T>(cconj<T>(e2), cmul_i<T>(cconj<T>(o2c))));
+}
+
 template <typename T, typename CF, typename DSINK>
 __device__ __forceinline__ void r2c_div_c2r_regs(T* buf, int c, int slot, bool partner_in_warp,
                                                  const LineTables<T>& tb, const DSINK& dv) {
@@ -226,44 +269,8 @@ __device__ __forceinline__ void r2c_div_c2r_regs(T* buf, int c, int slot, bool p
         for (int k = 0; k < R; ++k) u[k] = v[(k & 1) * 8 + (k >> 1)];
     }
 
-    // Pair (m, M - m) from Z[m] = zk, Z[M - m] = zm: the R2C split gives X[m]
-    // and X[M - m] (w^(M-m) = -conj w^m), each is divided by its eigenvalue,
-    // and the C2R pre step gives the inverse inputs at m (o1) and M - m (o2,
-    // the conjugate sums of o1's).  m = 0 pairs bin 0 with the Nyquist bin M.
     auto pair = [&](int m, C2<T> zk, C2<T> zm, C2<T>& o1, C2<T>& o2) {
-        const C2<T> wk = ldtw<T>(tb.twN + m);
-        if (m != 0 && 2 * m >= dv.dlo && 2 * m + 1 <= dv.dhi && N - 2 * m >= dv.dlo && N - 2 * m + 1 <= dv.dhi) {
-            // The split, the two divisions and the pre step compose into one
-            // real-linear map of (zk, zm).  With s = zk + conj zm,
-            // t = zk - conj zm, w = w^m = wr + i wi, dm, dp the reciprocal
-            // eigenvalues of bins m and M - m: X[m] = (s - i w t) / 2,
-            // X[M - m] = conj(s + i w t) / 2, and the pre step of the divided
-            // pair gives (|w| = 1)
-            //   o1 = ((dm + dp) + (dm - dp) wi) conj zk - i (dm - dp) wr zm
-            //   o2 = ((dm + dp) - (dm - dp) wi) conj zm - i (dm - dp) wr zk.
-            const T dm = (T)dv.eig(2 * m), dp = (T)dv.eig(N - 2 * m);
-            const T sum = dm + dp, dif = dm - dp;
-            const T c1 = sum + dif * wk.y, c2 = sum - dif * wk.y, g = dif * wk.x;
-            o1 = mk<T>(c1 * zk.x + g * zm.y, -(c1 * zk.y + g * zm.x));
-            o2 = mk<T>(c2 * zm.x + g * zk.y, -(c2 * zm.y + g * zk.x));
-            return;
-        }
-        const C2<T> e = cadd<T>(zk, cconj<T>(zm));
-        const C2<T> od = cmul<T>(wk, csub<T>(zk, cconj<T>(zm)));
-        C2<T> a = mk<T>(T(0.5) * (e.x + od.y), T(0.5) * (e.y - od.x));    // X[m]
-        C2<T> b = mk<T>(T(0.5) * (e.x - od.y), T(-0.5) * (e.y + od.x));   // X[M - m]
-        int lb = N - 2 * m;
-        if (m == 0) {
-            a = mk<T>(zk.x + zk.y, T(0));
-            b = mk<T>(zk.x - zk.y, T(0));
-            lb = N;
-        }
-        dv.div_pair(2 * m, a);
-        dv.div_pair(lb, b);
-        const C2<T> e2 = cadd<T>(a, cconj<T>(b));
-        const C2<T> o2c = cmul<T>(cconj<T>(wk), csub<T>(a, cconj<T>(b)));
-        o1 = cconj<T>(cadd<T>(e2, cmul_i<T>(o2c)));
-        o2 = cconj<T>(cadd<T>(cconj<T>(e2), cmul_i<T>(cconj<T>(o2c))));
+        split_div_pre<T, N>(m, zk, zm, o1, o2, tb, dv);
     };
 
     // Iteration k finishes bin k with its partner: lane ^ 16's u[15 - k]
@@ -304,6 +311,112 @@ __device__ __forceinline__ void r2c_div_c2r_regs(T* buf, int c, int slot, bool p
         r.y = __shfl_xor_sync(0xffffffffu, send[k].y, 16);
         if (partner_in_warp) u[R - 1 - k] = r;
     }
+
+    // inverse: stage 0 (inputs slot + P k = u[k]), exchange, stage 1, real
+    // outputs x[2m] = Re, x[2m+1] = -Im
+    fast::stage_compute<T, M, 0>(u, slot, tb.twM);
+#pragma unroll
+    for (int k = 0; k < R; ++k) Z[CF::zi(B0::out_idx(slot, 0, k), c)] = u[k];
+    CF::sync();
+#pragma unroll
+    for (int b = 0; b < B1::B; ++b)
+#pragma unroll
+        for (int k = 0; k < B1::r; ++k) u[b * B1::r + k] = Z[CF::zi(B1::in_idx(slot, b, k), c)];
+    CF::sync();
+    fast::stage_compute<T, M, 1>(u, slot, tb.twM);
+#pragma unroll
+    for (int b = 0; b < B1::B; ++b)
+#pragma unroll
+        for (int k = 0; k < B1::r; ++k) {
+            const int m = B1::out_idx(slot, b, k);
+            buf[(2 * m) * PR + c] = u[b * B1::r + k].x;
+            buf[(2 * m + 1) * PR + c] = -u[b * B1::r + k].y;
+        }
+}
+
+// The fused pass of N = 512 and 256 lines with 32-line tiles (FP32): one warp holds
+// one slot of all 32 lines, so a bin's partner M - m (held by slot P - slot)
+// is in another warp and the pair exchange goes through shared memory -- but
+// only the half of the spectrum the partners need: after the forward stages
+// (thread `slot` holds bins slot + P k, k = 0..15) every thread publishes its
+// bins k = 8..15, reads the partner bin of each of its k < 8, finishes both
+// bins of the pair, keeps its own and writes the partner's into the partner's
+// published slot, from which the partner reads its k = 8..15 back.  Slot 0
+// pairs with itself (bin 0 with the Nyquist bin, bin M / 2 alone), slot P / 2
+// too; the same reads and writes serve them.  The spectrum never makes the
+// full round trip of the unfused post / pre steps.
+template <typename T, int M, int WT, int KIND, int KIND2>
+struct SmemSpectrum {
+    static constexpr bool value = (M == 256 || M == 128) && WT == 32 && KIND == kR2C && KIND2 == kC2R;
+};
+
+template <typename T, typename CF, typename DSINK>
+__device__ __forceinline__ void r2c_div_c2r_smem(T* buf, int c, int slot, const LineTables<T>& tb,
+                                                 const DSINK& dv) {
+    constexpr int M = CF::M, N = CF::N, PR = CF::PR, P = CF::P;
+    static_assert((M == 256 || M == 128) && CF::W == 32, "M = 256 or 128, 32-line tiles");
+    using B0 = fast::Bfly<M, 0>;
+    using B1 = fast::Bfly<M, 1>;
+    constexpr int R = fast::kR;
+    const auto X = CF::reader(static_cast<const T*>(buf), c);
+    C2<T>* Z = reinterpret_cast<C2<T>*>(buf);
+    C2<T> u[R];
+
+    // forward: stage 0 with the pre step in the reads, exchange, stage 1
+#pragma unroll
+    for (int k = 0; k < R; ++k) u[k] = fast::pre_value<T, kR2C, M>(X, B0::in_idx(slot, 0, k), tb);
+    CF::sync();
+    fast::stage_compute<T, M, 0>(u, slot, tb.twM);
+#pragma unroll
+    for (int k = 0; k < R; ++k) Z[CF::zi(B0::out_idx(slot, 0, k), c)] = u[k];
+    CF::sync();
+    if constexpr (M == 256) {
+#pragma unroll
+        for (int k = 0; k < R; ++k) u[k] = Z[CF::zi(B1::in_idx(slot, 0, k), c)];
+        CF::sync();
+        fast::stage_compute<T, M, 1>(u, slot, tb.twM);
+    } else {
+        // radix 8 on butterflies j = slot + 8 b (as r2c_div_c2r_regs), so that
+        // this thread's outputs are bins slot + 8 k
+        static_assert(B1::r == 8 && B1::Ns == 16 && B1::nb == 16, "M = 128: last stage radix 8");
+        C2<T> v[R];
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[b * 8 + k] = Z[CF::zi(slot + 8 * b + 16 * k, c)];
+        CF::sync();
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const int j = slot + 8 * b;
+#pragma unroll
+            for (int k = 1; k < 8; ++k) v[b * 8 + k] = cmul<T>(v[b * 8 + k], ldtw<T>(tb.twM + j * k));
+            fast::dft_r<T, 8>(v + b * 8);
+        }
+#pragma unroll
+        for (int k = 0; k < R; ++k) u[k] = v[(k & 1) * 8 + (k >> 1)];
+    }
+    // u[k] = bin slot + P k; publish the upper half
+#pragma unroll
+    for (int k = R / 2; k < R; ++k) Z[CF::zi(slot + P * k, c)] = u[k];
+    CF::sync();
+#pragma unroll
+    for (int k = 0; k < R / 2; ++k) {
+        const int m = slot + P * k;
+        const C2<T> zm = (m == 0) ? u[0] : Z[CF::zi(M - m, c)];
+        C2<T> o1, o2;
+        split_div_pre<T, N>(m, u[k], zm, o1, o2, tb, dv);
+        u[k] = o1;
+        if (m != 0) Z[CF::zi(M - m, c)] = o2;
+    }
+    if (slot == 0) {   // bin M / 2 pairs with itself
+        C2<T> o1, o2;
+        split_div_pre<T, N>(M / 2, u[R / 2], u[R / 2], o1, o2, tb, dv);
+        Z[CF::zi(M / 2, c)] = o1;
+    }
+    CF::sync();
+#pragma unroll
+    for (int k = R / 2; k < R; ++k) u[k] = Z[CF::zi(slot + P * k, c)];
+    CF::sync();
 
     // inverse: stage 0 (inputs slot + P k = u[k]), exchange, stage 1, real
     // outputs x[2m] = Re, x[2m+1] = -Im
@@ -497,6 +610,8 @@ tma_pass(const __grid_constant__ CUtensorMap ldmap, const __grid_constant__ CUte
             s1.zmax = (a.dv.perturb && col <= a.dv.xz_hi && v <= a.dv.yz_hi) ? a.dv.zz_hi : -1;
             if constexpr (REGSPEC) {
                 r2c_div_c2r_regs<T, CF>(buf, c, slot, (t >> 5) != 0, tb, s1);
+            } else if constexpr (SmemSpectrum<T, M, W, KIND, KIND2>::value) {
+                r2c_div_c2r_smem<T, CF>(buf, c, slot, tb, s1);
             } else {
                 transform_lines<T, CF, KIND>(buf, red, c, slot, tb, s1);
                 OutSink<T, PR, false> s2;

@@ -53,6 +53,9 @@ def rel(a, b):
     ((48, 40, 56), (2, 1, 4), -7.5),      # mixed-radix kernels
     ((128, 32, 64), (4, 3, 2), -100.0),
     ((64, 64, 32), (1, 3, 0), -4.0),
+    ((40, 24, 512), (3, 4, 0), -1.0),     # periodic z at N = 512: fused FP32 z pass, pairs through shared memory
+    ((72, 8, 512), (1, 0, 0), -3.0),
+    ((24, 40, 256), (1, 3, 0), -4.0),     # the same at N = 256
 ])
 def test_refinement_reaches_fp64(dims, bcs, lam):
     p = gen.random_problem(*dims, *bcs, lam, seed=sum(dims) + 7 * sum(bcs))
