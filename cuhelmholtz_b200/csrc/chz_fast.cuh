@@ -21,6 +21,7 @@
 // the complex FFT view and the real output view; phases are separated by
 // barriers.
 #pragma once
+#include <type_traits>
 #include <utility>
 
 #include "chz_device.cuh"
@@ -68,9 +69,10 @@ template <> struct Plan<192> : MixedPlan<12, 12, 4, 4> {};
 
 // Geometry of a tile of W lines transformed by P = M/V threads each: the real
 // view of entry l of line c is buf[l * PR + c], the complex view of entry m is
-// Z[m * W + c].  BAR = 0 synchronises the CTA with __syncthreads; BAR > 0 uses
-// named barrier BAR over the NT compute threads only.
-template <int M_, int W_, int PR_, int BAR_>
+// Z[m * W + c] (rows permuted with ZPERM, below).  BAR = 0 synchronises the
+// CTA with __syncthreads; BAR > 0 uses named barrier BAR over the NT compute
+// threads only.
+template <int M_, int W_, int PR_, int BAR_, bool ZPERM = false>
 struct LineCfg {
     static constexpr int M = M_;
     static constexpr int V = Plan<M>::V;  // values per thread
@@ -93,13 +95,29 @@ struct LineCfg {
     __device__ static __forceinline__ StridedView<T> reader(const T* buf, int c) {
         return StridedView<T>{buf, PR, c};
     }
-    __device__ static __forceinline__ int zi(int m, int c) { return m * W + c; }
+    // ZPERM (8 lines, FP32): a row m of the exchange view is then half a bank
+    // cycle (8 x 8 bytes), and the four slot groups of a warp (slots w + 4 j in
+    // the contiguous passes) access rows of one parity, so they would share 16
+    // banks.  Rows m and m ^ 1 trade places when bits 2 and 6 of m differ: a
+    // permutation of the rows that puts two of the groups on each half for the
+    // stage exchanges (rows 16 slot + k written, slot + 16 k read) and the
+    // partner reads.  Measured faster only where the pass waits on shared
+    // memory (the accumulating FP32 x inverse: 0.686 -> 0.603 ms a launch under
+    // ncu); the issue-bound FP32 x forward from FP64 input slowed down with it
+    // (0.628 -> 0.795 ms), so only the former uses it.
+    __device__ static __forceinline__ int zi(int m, int c) {
+        if constexpr (ZPERM && W == 8) return (m ^ (((m >> 2) ^ (m >> 6)) & 1)) * W + c;
+        else return m * W + c;
+    }
 };
 
 // The persistent cp.async kernel: 128 threads, odd pitch W + 1 (conflict-free
 // transposed access).
 template <int M>
 using Cfg = LineCfg<M, kNT / (M / Plan<M>::V), kNT / (M / Plan<M>::V) + 1, 0>;
+// The same with the exchange rows permuted (the accumulating FP32 x inverse).
+template <int M>
+using CfgPerm = LineCfg<M, kNT / (M / Plan<M>::V), kNT / (M / Plan<M>::V) + 1, 0, true>;
 
 #define CHZ_C1 0.92387953251128675613
 #define CHZ_S1 0.38268343236508977173
@@ -630,7 +648,7 @@ template <typename T, typename TI, typename TO, int M, bool CONTIG, int KIND, in
 __device__ __forceinline__ void fast_tile(const TI* in, TO* out, const PassArgs& a, const LineTables<T>& tb,
                                           const double* ez_s, T* buf, T* red, int tile, int ntx, int t, int c,
                                           int slot, double* accb = nullptr) {
-    using CF = Cfg<M>;
+    using CF = std::conditional_t<acc_staged<T, TO, CONTIG>(), CfgPerm<M>, Cfg<M>>;
     constexpr int W = CF::W, PR = CF::PR, P = CF::P, N = CF::N;
     constexpr bool ACCS = acc_staged<T, TO, CONTIG>();
     const int tx = tile % ntx;
